@@ -1,0 +1,368 @@
+// Plain FP64 / ComplexF64 grouped block GEMM: one persistent launch for all coupled-sector
+// blocks of a TensorKit mul! (src/tensors/linalg.jl:330-370), tiles taken from a
+// cost-ordered device work queue (largest k first).
+//
+// Tensor path: FP64 DMMA (mma.sync.m8n8k4.f64). tcgen05 has no f64 kind, so the
+// double-precision tensor pipe is reached through DMMA; the split-precision path
+// (gemm_split.cu) is the tcgen05 one.
+//
+// CTA tile 64x64x16, 4 warps in a 2x2 grid (each 32x32 = 4x4 DMMA tiles), operands
+// double-buffered in shared memory with 8-byte cp.async (zero-filled outside the block,
+// so any lda/offset parity works). Complex blocks keep separate re/im planes and issue
+// four real DMMA per fragment pair.
+#include <algorithm>
+#include <cstring>
+
+#include "tkb_internal.h"
+
+namespace {
+
+constexpr int BM = 64, BN = 64, BK = 16;
+constexpr int APAD = 4, BPAD = 4;
+
+struct CDbl {
+  double x, y;
+};
+
+__device__ __forceinline__ void cp_async8(void *smem, const void *gmem, bool pred) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  const int sz = pred ? 8 : 0;
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(s), "l"(gmem), "r"(sz));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::); }
+__device__ __forceinline__ void cp_async_wait_1() { asm volatile("cp.async.wait_group 1;\n" ::); }
+
+__device__ __forceinline__ void dmma(double &c0, double &c1, double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+               : "+d"(c0), "+d"(c1)
+               : "d"(a), "d"(b));
+}
+
+// ---- real ----------------------------------------------------------------------------
+struct SmemR {
+  double A[2][BK][BM + APAD];
+  double B[2][BN][BK + BPAD];
+};
+
+__device__ __forceinline__ void load_tiles_r(SmemR &s, int buf, const GBlock &b, const double *A,
+                                             const double *B, int64_t m0, int64_t n0, int64_t k0) {
+  const int tid = threadIdx.x;
+  // A tile: op(A) rows m0.., cols k0..
+  if (b.opA == TKB_OP_N) {
+#pragma unroll
+    for (int r = 0; r < (BM * BK) / 128; ++r) {
+      const int e = tid + r * 128;
+      const int i = e % BM, l = e / BM;
+      const int64_t gi = m0 + i, gl = k0 + l;
+      const bool ok = gi < b.m && gl < b.k;
+      const double *p = A + b.offA + (ok ? gi + gl * b.lda : 0);
+      cp_async8(&s.A[buf][l][i], p, ok);
+    }
+  } else {
+#pragma unroll
+    for (int r = 0; r < (BM * BK) / 128; ++r) {
+      const int e = tid + r * 128;
+      const int l = e % BK, i = e / BK;
+      const int64_t gi = m0 + i, gl = k0 + l;
+      const bool ok = gi < b.m && gl < b.k;
+      const double *p = A + b.offA + (ok ? gl + gi * b.lda : 0);
+      cp_async8(&s.A[buf][l][i], p, ok);
+    }
+  }
+  if (b.opB == TKB_OP_N) {
+#pragma unroll
+    for (int r = 0; r < (BN * BK) / 128; ++r) {
+      const int e = tid + r * 128;
+      const int l = e % BK, j = e / BK;
+      const int64_t gl = k0 + l, gj = n0 + j;
+      const bool ok = gl < b.k && gj < b.n;
+      const double *p = B + b.offB + (ok ? gl + gj * b.ldb : 0);
+      cp_async8(&s.B[buf][j][l], p, ok);
+    }
+  } else {
+#pragma unroll
+    for (int r = 0; r < (BN * BK) / 128; ++r) {
+      const int e = tid + r * 128;
+      const int j = e % BN, l = e / BN;
+      const int64_t gl = k0 + l, gj = n0 + j;
+      const bool ok = gl < b.k && gj < b.n;
+      const double *p = B + b.offB + (ok ? gj + gl * b.ldb : 0);
+      cp_async8(&s.B[buf][j][l], p, ok);
+    }
+  }
+}
+
+__global__ void __launch_bounds__(128)
+    gemm_f64_kernel(const GBlock *__restrict__ blocks, const GTile *__restrict__ tiles, int ntiles,
+                    int *counters, double *__restrict__ C, const double *__restrict__ A,
+                    const double *__restrict__ B, double alpha, double beta) {
+  __shared__ __align__(16) SmemR s;
+  __shared__ int next_tile;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int wm = warp & 1, wn = warp >> 1;
+  const int g = lane >> 2, t = lane & 3;
+  while (true) {
+    if (threadIdx.x == 0) next_tile = atomicAdd(&counters[0], 1);
+    __syncthreads();
+    const int ti = next_tile;
+    __syncthreads();
+    if (ti >= ntiles) break;
+    const GTile tile = tiles[ti];
+    const GBlock b = blocks[tile.block];
+    const int64_t m0 = tile.m0, n0 = tile.n0;
+    double acc[4][4][2];
+#pragma unroll
+    for (int mi = 0; mi < 4; ++mi)
+#pragma unroll
+      for (int ni = 0; ni < 4; ++ni) acc[mi][ni][0] = acc[mi][ni][1] = 0.0;
+    const int64_t nk = (b.k + BK - 1) / BK;
+    if (nk > 0) {
+      load_tiles_r(s, 0, b, A, B, m0, n0, 0);
+      cp_async_commit();
+      for (int64_t kt = 0; kt < nk; ++kt) {
+        const int buf = kt & 1;
+        if (kt + 1 < nk) {
+          load_tiles_r(s, buf ^ 1, b, A, B, m0, n0, (kt + 1) * BK);
+          cp_async_commit();
+          cp_async_wait_1();
+        } else {
+          cp_async_wait_all();
+        }
+        __syncthreads();
+#pragma unroll
+        for (int kk = 0; kk < BK; kk += 4) {
+          double af[4], bf[4];
+#pragma unroll
+          for (int mi = 0; mi < 4; ++mi) af[mi] = s.A[buf][kk + t][wm * 32 + mi * 8 + g];
+#pragma unroll
+          for (int ni = 0; ni < 4; ++ni) bf[ni] = s.B[buf][wn * 32 + ni * 8 + g][kk + t];
+#pragma unroll
+          for (int mi = 0; mi < 4; ++mi)
+#pragma unroll
+            for (int ni = 0; ni < 4; ++ni) dmma(acc[mi][ni][0], acc[mi][ni][1], af[mi], bf[ni]);
+        }
+        __syncthreads();
+      }
+    }
+    // epilogue: C = α·acc + β·C
+#pragma unroll
+    for (int mi = 0; mi < 4; ++mi) {
+      const int64_t i = m0 + wm * 32 + mi * 8 + g;
+      if (i >= b.m) continue;
+#pragma unroll
+      for (int ni = 0; ni < 4; ++ni) {
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          const int64_t j = n0 + wn * 32 + ni * 8 + 2 * t + h;
+          if (j >= b.n) continue;
+          double *p = C + b.offC + i + j * b.ldc;
+          double r = alpha * acc[mi][ni][h];
+          if (beta != 0.0) r = fma(beta, *p, r);
+          *p = r;
+        }
+      }
+    }
+  }
+  // self-resetting queue: the last CTA out zeroes the counters for the next launch
+  if (threadIdx.x == 0) {
+    __threadfence();
+    const int done = atomicAdd(&counters[1], 1);
+    if (done == (int)gridDim.x - 1) {
+      atomicExch(&counters[0], 0);
+      atomicExch(&counters[1], 0);
+      __threadfence();
+    }
+  }
+}
+
+// ---- complex ---------------------------------------------------------------------------
+struct SmemC {
+  double Ar[2][BK][BM + APAD];
+  double Ai[2][BK][BM + APAD];
+  double Br[2][BN][BK + BPAD];
+  double Bi[2][BN][BK + BPAD];
+};
+
+__device__ __forceinline__ void load_tiles_c(SmemC &s, int buf, const GBlock &b, const double2 *A,
+                                             const double2 *B, int64_t m0, int64_t n0, int64_t k0) {
+  const int tid = threadIdx.x;  // 256 threads
+  const double *Ad = reinterpret_cast<const double *>(A);
+  const double *Bd = reinterpret_cast<const double *>(B);
+  if (b.opA == TKB_OP_N) {
+#pragma unroll
+    for (int r = 0; r < (BM * BK) / 256; ++r) {
+      const int e = tid + r * 256;
+      const int i = e % BM, l = e / BM;
+      const int64_t gi = m0 + i, gl = k0 + l;
+      const bool ok = gi < b.m && gl < b.k;
+      const int64_t idx = ok ? b.offA + gi + gl * b.lda : 0;
+      cp_async8(&s.Ar[buf][l][i], Ad + 2 * idx, ok);
+      cp_async8(&s.Ai[buf][l][i], Ad + 2 * idx + 1, ok);
+    }
+  } else {
+#pragma unroll
+    for (int r = 0; r < (BM * BK) / 256; ++r) {
+      const int e = tid + r * 256;
+      const int l = e % BK, i = e / BK;
+      const int64_t gi = m0 + i, gl = k0 + l;
+      const bool ok = gi < b.m && gl < b.k;
+      const int64_t idx = ok ? b.offA + gl + gi * b.lda : 0;
+      cp_async8(&s.Ar[buf][l][i], Ad + 2 * idx, ok);
+      cp_async8(&s.Ai[buf][l][i], Ad + 2 * idx + 1, ok);
+    }
+  }
+  if (b.opB == TKB_OP_N) {
+#pragma unroll
+    for (int r = 0; r < (BN * BK) / 256; ++r) {
+      const int e = tid + r * 256;
+      const int l = e % BK, j = e / BK;
+      const int64_t gl = k0 + l, gj = n0 + j;
+      const bool ok = gl < b.k && gj < b.n;
+      const int64_t idx = ok ? b.offB + gl + gj * b.ldb : 0;
+      cp_async8(&s.Br[buf][j][l], Bd + 2 * idx, ok);
+      cp_async8(&s.Bi[buf][j][l], Bd + 2 * idx + 1, ok);
+    }
+  } else {
+#pragma unroll
+    for (int r = 0; r < (BN * BK) / 256; ++r) {
+      const int e = tid + r * 256;
+      const int j = e % BN, l = e / BN;
+      const int64_t gl = k0 + l, gj = n0 + j;
+      const bool ok = gl < b.k && gj < b.n;
+      const int64_t idx = ok ? b.offB + gj + gl * b.ldb : 0;
+      cp_async8(&s.Br[buf][j][l], Bd + 2 * idx, ok);
+      cp_async8(&s.Bi[buf][j][l], Bd + 2 * idx + 1, ok);
+    }
+  }
+}
+
+__global__ void __launch_bounds__(256)
+    gemm_c128_kernel(const GBlock *__restrict__ blocks, const GTile *__restrict__ tiles, int ntiles,
+                     int *counters, double2 *__restrict__ C, const double2 *__restrict__ A,
+                     const double2 *__restrict__ B, CDbl alpha, CDbl beta) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  SmemC &s = *reinterpret_cast<SmemC *>(smem_raw);
+  __shared__ int next_tile;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;  // 8 warps: 2 (m) x 4 (n)
+  const int wm = warp & 1, wn = warp >> 1;                      // warp tile 32 x 16
+  const int g = lane >> 2, t = lane & 3;
+  const bool bz = beta.x == 0.0 && beta.y == 0.0;
+  while (true) {
+    if (threadIdx.x == 0) next_tile = atomicAdd(&counters[0], 1);
+    __syncthreads();
+    const int ti = next_tile;
+    __syncthreads();
+    if (ti >= ntiles) break;
+    const GTile tile = tiles[ti];
+    const GBlock b = blocks[tile.block];
+    // conjugation of an operand flips the sign of its imaginary plane
+    const double sa = (b.opA == TKB_OP_C) ? -1.0 : 1.0;
+    const double sb = (b.opB == TKB_OP_C) ? -1.0 : 1.0;
+    const int64_t m0 = tile.m0, n0 = tile.n0;
+    double ar[4][2][2], ai[4][2][2];
+#pragma unroll
+    for (int mi = 0; mi < 4; ++mi)
+#pragma unroll
+      for (int ni = 0; ni < 2; ++ni) ar[mi][ni][0] = ar[mi][ni][1] = ai[mi][ni][0] = ai[mi][ni][1] = 0.0;
+    const int64_t nk = (b.k + BK - 1) / BK;
+    if (nk > 0) {
+      load_tiles_c(s, 0, b, A, B, m0, n0, 0);
+      cp_async_commit();
+      for (int64_t kt = 0; kt < nk; ++kt) {
+        const int buf = kt & 1;
+        if (kt + 1 < nk) {
+          load_tiles_c(s, buf ^ 1, b, A, B, m0, n0, (kt + 1) * BK);
+          cp_async_commit();
+          cp_async_wait_1();
+        } else {
+          cp_async_wait_all();
+        }
+        __syncthreads();
+#pragma unroll
+        for (int kk = 0; kk < BK; kk += 4) {
+          double fr[4], fi[4], fin[4], gr[2], gi[2];
+#pragma unroll
+          for (int mi = 0; mi < 4; ++mi) {
+            fr[mi] = s.Ar[buf][kk + t][wm * 32 + mi * 8 + g];
+            fi[mi] = sa * s.Ai[buf][kk + t][wm * 32 + mi * 8 + g];
+            fin[mi] = -fi[mi];
+          }
+#pragma unroll
+          for (int ni = 0; ni < 2; ++ni) {
+            gr[ni] = s.Br[buf][wn * 16 + ni * 8 + g][kk + t];
+            gi[ni] = sb * s.Bi[buf][wn * 16 + ni * 8 + g][kk + t];
+          }
+#pragma unroll
+          for (int mi = 0; mi < 4; ++mi)
+#pragma unroll
+            for (int ni = 0; ni < 2; ++ni) {
+              dmma(ar[mi][ni][0], ar[mi][ni][1], fr[mi], gr[ni]);
+              dmma(ar[mi][ni][0], ar[mi][ni][1], fin[mi], gi[ni]);
+              dmma(ai[mi][ni][0], ai[mi][ni][1], fr[mi], gi[ni]);
+              dmma(ai[mi][ni][0], ai[mi][ni][1], fi[mi], gr[ni]);
+            }
+        }
+        __syncthreads();
+      }
+    }
+#pragma unroll
+    for (int mi = 0; mi < 4; ++mi) {
+      const int64_t i = m0 + wm * 32 + mi * 8 + g;
+      if (i >= b.m) continue;
+#pragma unroll
+      for (int ni = 0; ni < 2; ++ni) {
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          const int64_t j = n0 + wn * 16 + ni * 8 + 2 * t + h;
+          if (j >= b.n) continue;
+          double2 *p = C + b.offC + i + j * b.ldc;
+          const double vr = ar[mi][ni][h], vi = ai[mi][ni][h];
+          double rr = alpha.x * vr - alpha.y * vi;
+          double ri = alpha.x * vi + alpha.y * vr;
+          if (!bz) {
+            const double2 o = *p;
+            rr = fma(beta.x, o.x, fma(-beta.y, o.y, rr));
+            ri = fma(beta.x, o.y, fma(beta.y, o.x, ri));
+          }
+          *p = make_double2(rr, ri);
+        }
+      }
+    }
+  }
+  if (threadIdx.x == 0) {
+    __threadfence();
+    const int done = atomicAdd(&counters[1], 1);
+    if (done == (int)gridDim.x - 1) {
+      atomicExch(&counters[0], 0);
+      atomicExch(&counters[1], 0);
+      __threadfence();
+    }
+  }
+}
+
+}  // namespace
+
+int tkb_gemm_launch(tkb_ctx *ctx, const tkb_plan *p, void *C, const void *A, const void *B,
+                    tkb_scalar alpha, tkb_scalar beta) {
+  if (p->ntiles == 0) return TKB_OK;
+  if (p->dtype == TKB_F64) {
+    if (alpha.im != 0.0 || beta.im != 0.0)
+      return tkb_set_error(ctx, TKB_ERR_ARG, "complex scalar with real data");
+    const int grid = (int)std::min<int64_t>(p->ntiles, (int64_t)ctx->num_sms * 4);
+    gemm_f64_kernel<<<grid, 128, 0, ctx->stream>>>(p->blocks, p->tiles, (int)p->ntiles,
+                                                   ctx->counters, (double *)C, (const double *)A,
+                                                   (const double *)B, alpha.re, beta.re);
+  } else {
+    const int grid = (int)std::min<int64_t>(p->ntiles, (int64_t)ctx->num_sms * 2);
+    const size_t smem = sizeof(SmemC);
+    TKB_CUDA_TRY(ctx, cudaFuncSetAttribute(gemm_c128_kernel,
+                                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    gemm_c128_kernel<<<grid, 256, smem, ctx->stream>>>(
+        p->blocks, p->tiles, (int)p->ntiles, ctx->counters, (double2 *)C, (const double2 *)A,
+        (const double2 *)B, CDbl{alpha.re, alpha.im}, CDbl{beta.re, beta.im});
+  }
+  ctx->launches++;
+  TKB_CUDA_TRY(ctx, cudaGetLastError());
+  return TKB_OK;
+}

@@ -1,0 +1,134 @@
+// Internal declarations shared by the libtkb200 translation units.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cstdint>
+#include <cstdio>
+#include <string>
+#include <vector>
+
+#include "../../include/tkb200.h"
+
+struct tkb_ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  int num_sms = 148;
+  size_t smem_optin = 227 * 1024;
+  // scratch owned by the context (grown on demand, never shrunk before destroy)
+  void *ws = nullptr;
+  size_t ws_bytes = 0;
+  // device work-queue counters for persistent kernels (zeroed once, self-resetting)
+  int *counters = nullptr;
+  int64_t launches = 0;
+  std::string err;
+  cudaGraph_t capturing = nullptr;
+  bool in_capture = false;
+};
+
+// status helpers ------------------------------------------------------------------------
+int tkb_set_error(tkb_ctx *ctx, int code, const std::string &msg);
+#define TKB_CUDA_TRY(ctx, call)                                                            \
+  do {                                                                                     \
+    cudaError_t _e = (call);                                                               \
+    if (_e != cudaSuccess)                                                                 \
+      return tkb_set_error((ctx), TKB_ERR_CUDA,                                            \
+                           std::string(#call) + ": " + cudaGetErrorString(_e));            \
+  } while (0)
+
+int tkb_ensure_workspace(tkb_ctx *ctx, size_t bytes);
+
+// tree transform ------------------------------------------------------------------------
+struct TGroup {
+  int32_t ndim;        // canonical dims (after squeezing size-1 dims and merging)
+  int32_t da, db;      // tile dims (canonical indices)
+  int32_t ta, tb;      // tile extents
+  int32_t mode;        // 0 = copy (da fast on both sides), 1 = transpose through smem
+  int32_t nouter;
+  int32_t outer[TKB_MAX_IND];
+  int64_t size[TKB_MAX_IND];
+  int64_t ntile_a, ntile_b;
+  int64_t task_begin;
+  int64_t src_tree_begin, nsrc, dst_tree_begin, ndst, coeff_begin;
+};
+
+struct tkb_table {
+  tkb_ctx *owner = nullptr;
+  int ngroups = 0;
+  int64_t ntasks = 0;
+  int64_t elems_read = 0, elems_written = 0;
+  int max_trees = 1;             // max(nsrc) over groups
+  size_t smem_f64 = 0;           // dynamic smem bytes needed for f64
+  size_t smem_c128 = 0;
+  int64_t src_len = 0, dst_len = 0;
+  // device arrays
+  TGroup *groups = nullptr;
+  int64_t *sstr = nullptr, *soff = nullptr, *dstr = nullptr, *doff = nullptr;
+  double *coeffs = nullptr;
+  int64_t *task_begin = nullptr;  // ngroups, for the device-side group lookup
+};
+
+int tkb_transform_launch(tkb_ctx *ctx, const tkb_table *t, int dtype, void *dst,
+                         const void *src, tkb_scalar alpha, tkb_scalar beta, int conj);
+
+// grouped gemm --------------------------------------------------------------------------
+struct GBlock {
+  int64_t m, n, k;
+  int64_t offA, offB, offC;
+  int64_t lda, ldb, ldc;
+  int32_t opA, opB;
+  // split precision: workspace offsets of the sliced operands and exponents
+  int64_t wsA, wsB, wsEA, wsEB;
+  int32_t mpad, npad, kpad;   // padded extents (tile multiples) of the sliced operands
+  int32_t pad_;
+};
+
+struct GTile {
+  int32_t block;
+  int32_t m0, n0;
+  int32_t kind;  // 0 = gemm tile, 1 = β-scale only (k == 0)
+};
+
+struct tkb_plan {
+  tkb_ctx *owner = nullptr;
+  int dtype = 0, precision = 0, slices = 0;
+  int64_t nblocks = 0, ntiles = 0;
+  double flops = 0;
+  int64_t lenA = 0, lenB = 0, lenC = 0;
+  std::vector<GBlock> hblocks;
+  GBlock *blocks = nullptr;
+  GTile *tiles = nullptr;
+  // split precision
+  size_t ws_bytes = 0;          // workspace needed for slices + exponents
+  int64_t slice_rows_A = 0, slice_rows_B = 0;  // total padded rows for the slicing pass
+  GTile *stiles = nullptr;      // tiles of the split kernel (different tile shape)
+  int64_t nstiles = 0;
+  void *sjobs = nullptr;        // slice jobs (block, operand)
+  int64_t *srow_begin = nullptr;
+  int nsjobs = 0;
+  int64_t nsrows = 0;
+  int tile_m = 64, tile_n = 64;
+};
+
+int tkb_gemm_launch(tkb_ctx *ctx, const tkb_plan *p, void *C, const void *A, const void *B,
+                    tkb_scalar alpha, tkb_scalar beta);
+int tkb_gemm_split_prepare(tkb_ctx *ctx, tkb_plan *p);
+int tkb_gemm_split_launch(tkb_ctx *ctx, const tkb_plan *p, void *C, const void *A,
+                          const void *B, tkb_scalar alpha, tkb_scalar beta);
+
+// reductions ----------------------------------------------------------------------------
+struct RSeg {
+  int64_t off, count, stride;
+  double weight;
+};
+
+struct tkb_rplan {
+  tkb_ctx *owner = nullptr;
+  int64_t nseg = 0;
+  int64_t total = 0;
+  RSeg *segs = nullptr;
+  int64_t *seg_begin = nullptr;  // prefix sums of counts (device)
+  int nblocks_launch = 0;
+};
+
+int tkb_reduce_launch(tkb_ctx *ctx, const tkb_rplan *p, int kind, int dtype, const void *x,
+                      const void *y, double *dev_out);

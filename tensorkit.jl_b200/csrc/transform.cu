@@ -1,0 +1,467 @@
+// Tree transform: gather-permute-recouple-scale-scatter of all sub-blocks of one
+// permute/braid in a single launch.
+//
+// Semantics (TensorKit add_transform_kernel!, src/tensors/indexmanipulations.jl:658-726):
+//   for every group g (a fusion block, or one abelian tree pair):
+//     dst_i = β·dst_i + α·Σ_j U_g[i,j] · permutedims(src_j, perm)      i < ndst_g, j < nsrc_g
+// A group's sub-blocks share their sizes; only strides/offsets differ per tree.
+//
+// Work decomposition: every group is canonicalised on the host (size-1 dims removed,
+// dims contiguous on both sides merged) and tiled over two dims (a, b):
+//   copy mode      a is the fastest dim of both source and destination: loads and stores
+//                  are coalesced along a, source tiles staged in shared memory only when
+//                  the group recouples several trees;
+//   transpose mode a is the destination's fastest dim, b the source's: the source tile is
+//                  read coalesced along b into shared memory (row pitch tb+1 to avoid bank
+//                  conflicts) and written coalesced along a.
+// All remaining dims are "outer": one task = one (tile_a, tile_b, outer index) of a group.
+// Tasks of all groups form one grid; groups arrive sorted by decreasing weight.
+#include <algorithm>
+#include <cstring>
+#include <numeric>
+
+#include "tkb_internal.h"
+
+namespace {
+
+constexpr int kThreads = 256;
+constexpr size_t kSmemBudget = 96 * 1024;
+
+struct CDbl {
+  double x, y;
+};
+
+__device__ __forceinline__ double ld_val(const double *p, bool) { return __ldg(p); }
+__device__ __forceinline__ double2 ld_val(const double2 *p, bool conj) {
+  double2 v = __ldg(p);
+  if (conj) v.y = -v.y;
+  return v;
+}
+__device__ __forceinline__ double zero_val(double) { return 0.0; }
+__device__ __forceinline__ double2 zero_val(double2) { return make_double2(0.0, 0.0); }
+__device__ __forceinline__ double axpy_r(double u, double v, double acc) { return fma(u, v, acc); }
+__device__ __forceinline__ double2 axpy_r(double u, double2 v, double2 acc) {
+  return make_double2(fma(u, v.x, acc.x), fma(u, v.y, acc.y));
+}
+// out = α·v + β·d   (β_zero: d not read)
+__device__ __forceinline__ double finish(double v, double a, double b, const double *d,
+                                         bool bz) {
+  double r = a * v;
+  if (!bz) r = fma(b, *d, r);
+  return r;
+}
+__device__ __forceinline__ double2 finish(double2 v, double2 a, double2 b, const double2 *d,
+                                          bool bz) {
+  double2 r = make_double2(a.x * v.x - a.y * v.y, a.x * v.y + a.y * v.x);
+  if (!bz) {
+    double2 o = *d;
+    r.x = fma(b.x, o.x, fma(-b.y, o.y, r.x));
+    r.y = fma(b.x, o.y, fma(b.y, o.x, r.y));
+  }
+  return r;
+}
+
+template <typename T>
+__device__ __forceinline__ T scalar_from(CDbl s);
+template <>
+__device__ __forceinline__ double scalar_from<double>(CDbl s) { return s.x; }
+template <>
+__device__ __forceinline__ double2 scalar_from<double2>(CDbl s) { return make_double2(s.x, s.y); }
+
+template <typename T, bool CONJ>
+__global__ void __launch_bounds__(kThreads)
+    treetransform_kernel(const TGroup *__restrict__ groups, const int64_t *__restrict__ task_begin,
+                         int ngroups, int64_t ntasks, const int64_t *__restrict__ sstr,
+                         const int64_t *__restrict__ soff, const int64_t *__restrict__ dstr,
+                         const int64_t *__restrict__ doff, const double *__restrict__ coeffs,
+                         T *__restrict__ dst, const T *__restrict__ src, CDbl alpha_, CDbl beta_,
+                         int beta_zero) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T *sm = reinterpret_cast<T *>(smem_raw);
+  const T alpha = scalar_from<T>(alpha_);
+  const T beta = scalar_from<T>(beta_);
+  const bool bz = beta_zero != 0;
+
+  for (int64_t task = blockIdx.x; task < ntasks; task += gridDim.x) {
+    // locate the group: last g with task_begin[g] <= task
+    int lo = 0, hi = ngroups - 1;
+    while (lo < hi) {
+      int mid = (lo + hi + 1) >> 1;
+      if (task_begin[mid] <= task) lo = mid; else hi = mid - 1;
+    }
+    const TGroup &G = groups[lo];
+    int64_t t = task - G.task_begin;
+    const int64_t itb = t % G.ntile_b;
+    t /= G.ntile_b;
+    const int64_t ita = t % G.ntile_a;
+    int64_t o = t / G.ntile_a;
+    // outer multi-index -> per-tree base offsets computed lazily below
+    int64_t oidx[TKB_MAX_IND];
+#pragma unroll
+    for (int q = 0; q < TKB_MAX_IND; ++q) {
+      if (q < G.nouter) {
+        const int64_t s = G.size[G.outer[q]];
+        oidx[q] = o % s;
+        o /= s;
+      }
+    }
+    const int da = G.da, db = G.db;
+    const int ta = G.ta, tb = G.tb;
+    const int64_t a0 = ita * ta, b0 = itb * tb;
+    const int64_t sa = G.size[da];
+    const int64_t sb = db >= 0 ? G.size[db] : 1;
+    const int na = (int)(sa - a0 < ta ? sa - a0 : ta);
+    const int nb = (int)(sb - b0 < tb ? sb - b0 : tb);
+    const int nel = na * nb;
+    const int64_t nsrc = G.nsrc, ndst = G.ndst;
+
+    auto src_base = [&](int64_t j) {
+      const int64_t *st = sstr + (G.src_tree_begin + j) * TKB_MAX_IND;
+      int64_t off = soff[G.src_tree_begin + j] + a0 * st[da] + (db >= 0 ? b0 * st[db] : 0);
+      for (int q = 0; q < G.nouter; ++q) off += oidx[q] * st[G.outer[q]];
+      return off;
+    };
+    auto dst_base = [&](int64_t i) {
+      const int64_t *st = dstr + (G.dst_tree_begin + i) * TKB_MAX_IND;
+      int64_t off = doff[G.dst_tree_begin + i] + a0 * st[da] + (db >= 0 ? b0 * st[db] : 0);
+      for (int q = 0; q < G.nouter; ++q) off += oidx[q] * st[G.outer[q]];
+      return off;
+    };
+
+    if (G.mode == 0 && nsrc == 1 && ndst == 1) {
+      // direct copy: coalesced along a on both sides
+      const int64_t *ss = sstr + G.src_tree_begin * TKB_MAX_IND;
+      const int64_t *ds = dstr + G.dst_tree_begin * TKB_MAX_IND;
+      const int64_t sA = ss[da], dA = ds[da];
+      const int64_t sB = db >= 0 ? ss[db] : 0, dB = db >= 0 ? ds[db] : 0;
+      const int64_t sb0 = src_base(0), db0 = dst_base(0);
+      const double u = coeffs[G.coeff_begin];
+      for (int e = threadIdx.x; e < nel; e += kThreads) {
+        const int ia = e % na, ib = e / na;
+        T v = ld_val(src + sb0 + ia * sA + ib * sB, CONJ);
+        T acc = axpy_r(u, v, zero_val(v));
+        T *dp = dst + db0 + ia * dA + ib * dB;
+        *dp = finish(acc, alpha, beta, dp, bz);
+      }
+      continue;
+    }
+
+    // staged path: all source tiles of the group into shared memory
+    const int pitch = (G.mode == 1) ? (tb + 1) : 0;
+    const int tile_elems = (G.mode == 1) ? ta * (tb + 1) : ta * tb;
+    for (int64_t j = 0; j < nsrc; ++j) {
+      const int64_t *ss = sstr + (G.src_tree_begin + j) * TKB_MAX_IND;
+      const int64_t sA = ss[da], sB = db >= 0 ? ss[db] : 0;
+      const int64_t base = src_base(j);
+      T *tile = sm + j * tile_elems;
+      if (G.mode == 1) {
+        for (int e = threadIdx.x; e < nel; e += kThreads) {
+          const int ib = e % nb, ia = e / nb;  // b fastest: coalesced source reads
+          tile[ia * pitch + ib] = ld_val(src + base + ia * sA + ib * sB, CONJ);
+        }
+      } else {
+        for (int e = threadIdx.x; e < nel; e += kThreads) {
+          const int ia = e % na, ib = e / na;
+          tile[ib * ta + ia] = ld_val(src + base + ia * sA + ib * sB, CONJ);
+        }
+      }
+    }
+    __syncthreads();
+    const double *U = coeffs + G.coeff_begin;
+    for (int64_t i = 0; i < ndst; ++i) {
+      const int64_t *ds = dstr + (G.dst_tree_begin + i) * TKB_MAX_IND;
+      const int64_t dA = ds[da], dB = db >= 0 ? ds[db] : 0;
+      const int64_t base = dst_base(i);
+      const double *Ui = U + i * nsrc;
+      for (int e = threadIdx.x; e < nel; e += kThreads) {
+        const int ia = e % na, ib = e / na;  // a fastest: coalesced destination writes
+        const int sidx = (G.mode == 1) ? ia * pitch + ib : ib * ta + ia;
+        T acc = zero_val(T{});
+        for (int64_t j = 0; j < nsrc; ++j) acc = axpy_r(Ui[j], sm[j * tile_elems + sidx], acc);
+        T *dp = dst + base + ia * dA + ib * dB;
+        *dp = finish(acc, alpha, beta, dp, bz);
+      }
+    }
+    __syncthreads();
+  }
+}
+
+int64_t pow2ceil(int64_t x) {
+  int64_t p = 1;
+  while (p < x) p <<= 1;
+  return p;
+}
+
+}  // namespace
+
+extern "C" int tkb_table_create(tkb_ctx *ctx, const tkb_table_desc *d, tkb_table **out) {
+  if (!ctx || !d || !out) return TKB_ERR_ARG;
+  *out = nullptr;
+  const int N = d->nind;
+  if (N < 0 || N > TKB_MAX_IND) return tkb_set_error(ctx, TKB_ERR_ARG, "nind out of range");
+  if (d->ngroups < 0) return tkb_set_error(ctx, TKB_ERR_ARG, "negative ngroups");
+  {
+    std::vector<int> seen(N, 0);
+    for (int k = 0; k < N; ++k) {
+      if (d->perm[k] < 0 || d->perm[k] >= N || seen[d->perm[k]]++)
+        return tkb_set_error(ctx, TKB_ERR_ARG, "perm is not a permutation");
+    }
+  }
+  const int64_t G = d->ngroups;
+  if (G > 0 && (!d->group_src_ptr || !d->group_dst_ptr || !d->coeff_ptr || !d->coeffs ||
+                (N > 0 && (!d->sizes || !d->src_strides || !d->dst_strides)) ||
+                !d->src_offsets || !d->dst_offsets))
+    return tkb_set_error(ctx, TKB_ERR_ARG, "null table array");
+
+  std::vector<TGroup> hg;
+  hg.reserve(G);
+  std::vector<int64_t> hsstr, hsoff, hdstr, hdoff, htask;
+  std::vector<double> hcoef;
+  int64_t ntasks = 0, er = 0, ew = 0;
+  size_t smem_max_f64 = 0, smem_max_c128 = 0;
+  int max_trees = 1;
+
+  for (int64_t g = 0; g < G; ++g) {
+    const int64_t s0 = d->group_src_ptr[g], s1 = d->group_src_ptr[g + 1];
+    const int64_t t0 = d->group_dst_ptr[g], t1 = d->group_dst_ptr[g + 1];
+    const int64_t c0 = d->coeff_ptr[g], c1 = d->coeff_ptr[g + 1];
+    const int64_t nsrc = s1 - s0, ndst = t1 - t0;
+    if (nsrc <= 0 || ndst <= 0 || c1 - c0 != nsrc * ndst)
+      return tkb_set_error(ctx, TKB_ERR_ARG, "inconsistent group pointers");
+    const int64_t *sz = d->sizes + g * N;
+    int64_t vol = 1;
+    for (int k = 0; k < N; ++k) {
+      if (sz[k] <= 0) return tkb_set_error(ctx, TKB_ERR_SIZE, "non-positive sub-block size");
+      vol *= sz[k];
+    }
+    // bounds validation of every tree (prevents any out-of-range device access)
+    for (int64_t j = s0; j < s1; ++j) {
+      int64_t hi = d->src_offsets[j];
+      if (hi < 0) return tkb_set_error(ctx, TKB_ERR_SIZE, "negative source offset");
+      for (int k = 0; k < N; ++k) {
+        const int64_t st = d->src_strides[j * N + k];
+        if (st < 0) return tkb_set_error(ctx, TKB_ERR_SIZE, "negative source stride");
+        hi += (sz[k] - 1) * st;
+      }
+      if (hi >= d->src_len)
+        return tkb_set_error(ctx, TKB_ERR_SIZE, "source sub-block exceeds source data length");
+    }
+    for (int64_t i = t0; i < t1; ++i) {
+      int64_t hi = d->dst_offsets[i];
+      if (hi < 0) return tkb_set_error(ctx, TKB_ERR_SIZE, "negative destination offset");
+      for (int k = 0; k < N; ++k) {
+        const int64_t st = d->dst_strides[i * N + k];
+        if (st < 0) return tkb_set_error(ctx, TKB_ERR_SIZE, "negative destination stride");
+        hi += (sz[d->perm[k]] - 1) * st;
+      }
+      if (hi >= d->dst_len)
+        return tkb_set_error(ctx, TKB_ERR_SIZE,
+                             "destination sub-block exceeds destination data length");
+    }
+    er += vol * nsrc;
+    ew += vol * ndst;
+
+    // canonical dims in destination order: (size, src strides per tree, dst strides per tree)
+    struct Dim {
+      int64_t size;
+      std::vector<int64_t> ss, ds;
+    };
+    std::vector<Dim> dims;
+    for (int k = 0; k < N; ++k) {
+      const int ks = d->perm[k];
+      if (sz[ks] == 1) continue;
+      Dim dm;
+      dm.size = sz[ks];
+      for (int64_t j = s0; j < s1; ++j) dm.ss.push_back(d->src_strides[j * N + ks]);
+      for (int64_t i = t0; i < t1; ++i) dm.ds.push_back(d->dst_strides[i * N + k]);
+      dims.push_back(dm);
+    }
+    // merge neighbours contiguous on both sides for every tree
+    for (size_t k = 0; k + 1 < dims.size();) {
+      bool ok = true;
+      for (size_t j = 0; j < dims[k].ss.size() && ok; ++j)
+        ok = dims[k + 1].ss[j] == dims[k].ss[j] * dims[k].size;
+      for (size_t i = 0; i < dims[k].ds.size() && ok; ++i)
+        ok = dims[k + 1].ds[i] == dims[k].ds[i] * dims[k].size;
+      if (ok) {
+        dims[k].size *= dims[k + 1].size;
+        dims.erase(dims.begin() + k + 1);
+      } else {
+        ++k;
+      }
+    }
+    if (dims.empty()) {  // scalar sub-block
+      Dim dm;
+      dm.size = 1;
+      dm.ss.assign(nsrc, 1);
+      dm.ds.assign(ndst, 1);
+      dims.push_back(dm);
+    }
+    const int nd = (int)dims.size();
+    TGroup tg;
+    std::memset(&tg, 0, sizeof(tg));
+    tg.ndim = nd;
+    for (int k = 0; k < nd; ++k) tg.size[k] = dims[k].size;
+    // fastest dims (tree 0 pattern; all trees of a group share it)
+    int fa = 0, fs = 0;
+    for (int k = 1; k < nd; ++k) {
+      if (dims[k].ds[0] < dims[fa].ds[0]) fa = k;
+      if (dims[k].ss[0] < dims[fs].ss[0]) fs = k;
+    }
+    const size_t el64 = 8, el128 = 16;
+    int64_t ta, tb;
+    int db;
+    if (fa == fs) {
+      tg.mode = 0;
+      db = -1;
+      int64_t best = 0;
+      for (int k = 0; k < nd; ++k)
+        if (k != fa && dims[k].size > best) { best = dims[k].size; db = k; }
+      ta = std::min<int64_t>(pow2ceil(dims[fa].size), 1024);
+      tb = db >= 0 ? std::min<int64_t>(pow2ceil(dims[db].size), std::max<int64_t>(1, 1024 / ta)) : 1;
+      // shared-memory budget when several trees are staged
+      while (nsrc > 1 && (size_t)(nsrc * ta * tb) * el128 > kSmemBudget && (ta > 1 || tb > 1)) {
+        if (tb > 1) tb >>= 1; else ta >>= 1;
+      }
+    } else {
+      tg.mode = 1;
+      db = fs;
+      ta = std::min<int64_t>(pow2ceil(dims[fa].size), 32);
+      tb = std::min<int64_t>(pow2ceil(dims[db].size), 32);
+      while (ta * tb < 1024) {
+        const bool grow_a = ta < dims[fa].size && (ta <= tb || tb >= dims[db].size);
+        const bool grow_b = tb < dims[db].size;
+        if (grow_a && ta < 256) ta <<= 1;
+        else if (grow_b && tb < 256) tb <<= 1;
+        else break;
+      }
+      while ((size_t)(nsrc * ta * (tb + 1)) * el128 > kSmemBudget && (ta > 1 || tb > 1)) {
+        if (ta >= tb && ta > 1) ta >>= 1; else tb >>= 1;
+      }
+    }
+    tg.da = fa;
+    tg.db = db;
+    tg.ta = (int)ta;
+    tg.tb = (int)tb;
+    tg.nouter = 0;
+    int64_t nouter_total = 1;
+    for (int k = 0; k < nd; ++k) {
+      if (k == fa || k == db) continue;
+      tg.outer[tg.nouter++] = k;
+      nouter_total *= dims[k].size;
+    }
+    tg.ntile_a = (dims[fa].size + ta - 1) / ta;
+    tg.ntile_b = db >= 0 ? (dims[db].size + tb - 1) / tb : 1;
+    tg.task_begin = ntasks;
+    ntasks += tg.ntile_a * tg.ntile_b * nouter_total;
+    tg.src_tree_begin = (int64_t)hsoff.size();
+    tg.dst_tree_begin = (int64_t)hdoff.size();
+    tg.nsrc = nsrc;
+    tg.ndst = ndst;
+    tg.coeff_begin = (int64_t)hcoef.size();
+    for (int64_t j = 0; j < nsrc; ++j) {
+      hsoff.push_back(d->src_offsets[s0 + j]);
+      for (int k = 0; k < TKB_MAX_IND; ++k) hsstr.push_back(k < nd ? dims[k].ss[j] : 0);
+    }
+    for (int64_t i = 0; i < ndst; ++i) {
+      hdoff.push_back(d->dst_offsets[t0 + i]);
+      for (int k = 0; k < TKB_MAX_IND; ++k) hdstr.push_back(k < nd ? dims[k].ds[i] : 0);
+    }
+    for (int64_t c = c0; c < c1; ++c) hcoef.push_back(d->coeffs[c]);
+    const bool staged = !(tg.mode == 0 && nsrc == 1 && ndst == 1);
+    if (staged) {
+      const int64_t te = tg.mode == 1 ? ta * (tb + 1) : ta * tb;
+      smem_max_f64 = std::max(smem_max_f64, (size_t)(nsrc * te) * el64);
+      smem_max_c128 = std::max(smem_max_c128, (size_t)(nsrc * te) * el128);
+    }
+    max_trees = std::max<int>(max_trees, (int)nsrc);
+    htask.push_back(tg.task_begin);
+    hg.push_back(tg);
+  }
+  if (std::max(smem_max_f64, smem_max_c128) > ctx->smem_optin)
+    return tkb_set_error(ctx, TKB_ERR_UNSUPPORTED, "fusion block too large for shared memory");
+
+  tkb_table *t = new tkb_table();
+  t->owner = ctx;
+  t->ngroups = (int)G;
+  t->ntasks = ntasks;
+  t->elems_read = er;
+  t->elems_written = ew;
+  t->max_trees = max_trees;
+  t->smem_f64 = smem_max_f64;
+  t->smem_c128 = smem_max_c128;
+  t->src_len = d->src_len;
+  t->dst_len = d->dst_len;
+  auto up = [&](void **dptr, const void *h, size_t bytes) -> cudaError_t {
+    if (bytes == 0) return cudaSuccess;
+    cudaError_t e = cudaMalloc(dptr, bytes);
+    if (e != cudaSuccess) return e;
+    return cudaMemcpy(*dptr, h, bytes, cudaMemcpyHostToDevice);
+  };
+  cudaError_t e = cudaSetDevice(ctx->device);
+  if (e == cudaSuccess) e = up((void **)&t->groups, hg.data(), hg.size() * sizeof(TGroup));
+  if (e == cudaSuccess) e = up((void **)&t->task_begin, htask.data(), htask.size() * 8);
+  if (e == cudaSuccess) e = up((void **)&t->sstr, hsstr.data(), hsstr.size() * 8);
+  if (e == cudaSuccess) e = up((void **)&t->soff, hsoff.data(), hsoff.size() * 8);
+  if (e == cudaSuccess) e = up((void **)&t->dstr, hdstr.data(), hdstr.size() * 8);
+  if (e == cudaSuccess) e = up((void **)&t->doff, hdoff.data(), hdoff.size() * 8);
+  if (e == cudaSuccess) e = up((void **)&t->coeffs, hcoef.data(), hcoef.size() * 8);
+  if (e != cudaSuccess) {
+    tkb_table_destroy(t);
+    return tkb_set_error(ctx, e == cudaErrorMemoryAllocation ? TKB_ERR_OOM : TKB_ERR_CUDA,
+                         std::string("table upload: ") + cudaGetErrorString(e));
+  }
+  *out = t;
+  return TKB_OK;
+}
+
+extern "C" int tkb_table_destroy(tkb_table *t) {
+  if (!t) return TKB_OK;
+  cudaFree(t->groups);
+  cudaFree(t->task_begin);
+  cudaFree(t->sstr);
+  cudaFree(t->soff);
+  cudaFree(t->dstr);
+  cudaFree(t->doff);
+  cudaFree(t->coeffs);
+  delete t;
+  return TKB_OK;
+}
+
+extern "C" int tkb_table_info(const tkb_table *t, int64_t *ntasks, int64_t *er, int64_t *ew) {
+  if (!t) return TKB_ERR_ARG;
+  if (ntasks) *ntasks = t->ntasks;
+  if (er) *er = t->elems_read;
+  if (ew) *ew = t->elems_written;
+  return TKB_OK;
+}
+
+int tkb_transform_launch(tkb_ctx *ctx, const tkb_table *t, int dtype, void *dst,
+                         const void *src, tkb_scalar alpha, tkb_scalar beta, int conj) {
+  if (t->ntasks == 0) return TKB_OK;
+  const int grid = (int)std::min<int64_t>(t->ntasks, (int64_t)ctx->num_sms * 16);
+  CDbl a{alpha.re, alpha.im}, b{beta.re, beta.im};
+  const int bz = (beta.re == 0.0 && beta.im == 0.0) ? 1 : 0;
+  if (dtype == TKB_F64) {
+    if (alpha.im != 0.0 || beta.im != 0.0)
+      return tkb_set_error(ctx, TKB_ERR_ARG, "complex scalar with real data");
+    const size_t smem = t->smem_f64;
+    auto k = treetransform_kernel<double, false>;
+    if (smem > 48 * 1024) TKB_CUDA_TRY(ctx, cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    k<<<grid, kThreads, smem, ctx->stream>>>(t->groups, t->task_begin, t->ngroups, t->ntasks,
+                                            t->sstr, t->soff, t->dstr, t->doff, t->coeffs,
+                                            (double *)dst, (const double *)src, a, b, bz);
+  } else if (dtype == TKB_C128) {
+    const size_t smem = t->smem_c128;
+    auto k = conj ? treetransform_kernel<double2, true> : treetransform_kernel<double2, false>;
+    if (smem > 48 * 1024) TKB_CUDA_TRY(ctx, cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    k<<<grid, kThreads, smem, ctx->stream>>>(t->groups, t->task_begin, t->ngroups, t->ntasks,
+                                            t->sstr, t->soff, t->dstr, t->doff, t->coeffs,
+                                            (double2 *)dst, (const double2 *)src, a, b, bz);
+  } else {
+    return tkb_set_error(ctx, TKB_ERR_ARG, "unknown dtype");
+  }
+  ctx->launches++;
+  TKB_CUDA_TRY(ctx, cudaGetLastError());
+  return TKB_OK;
+}

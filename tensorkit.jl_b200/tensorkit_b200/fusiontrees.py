@@ -1,0 +1,405 @@
+"""Fusion trees, fusion-tree blocks and the recoupling moves of the permute/braid path.
+
+Follows, for multiplicity-free sectors (U1, SU2, U1⊠SU2):
+- `FusionTree` / `FusionTreeBlock` (`src/fusiontrees/fusiontrees.jl:22-157`);
+- the deterministic iteration order (`src/fusiontrees/iterator.jl:98-226`);
+- `bendright` / `bendleft` and `repartition` (`src/fusiontrees/duality_manipulations.jl:33-194`,
+  `:460-505`);
+- `artin_braid` for single trees (`src/fusiontrees/braiding_manipulations.jl:18-79`) and for
+  blocks (`:81-198`), `braid` of a unique-fusion tree (`:215-251`), `fsbraid` (`:304-340`);
+- `linearizepermutation` and `permutation2swaps` (`src/auxiliary/auxiliary.jl:1-28`).
+
+Unique fusion (U1) uses single tree pairs and scalar coefficients; multiplicity-free
+non-abelian fusion (SU2, U1⊠SU2) uses FusionTreeBlocks and recoupling matrices U with
+`U = U_tmp @ U` accumulated in the reference's order.
+"""
+from __future__ import annotations
+
+from functools import lru_cache
+
+import numpy as np
+
+from .sectors import (Bsymbol, Fsymbol, Nsymbol, Rsymbol, frobenius_schur_phase,
+                      invsqrtdim, otimes_many, sqrtdim)
+
+__all__ = ["FusionTree", "FusionTreeBlock", "fusiontrees", "bendright", "bendleft",
+           "repartition", "artin_braid", "braid", "permute", "linearizepermutation",
+           "permutation2swaps"]
+
+
+class FusionTree:
+    """Splitting tree: coupled → uncoupled[0] ⊗ ... ⊗ uncoupled[N-1] (multiplicity-free)."""
+    __slots__ = ("uncoupled", "coupled", "isdual", "innerlines", "_h")
+
+    def __init__(self, uncoupled, coupled, isdual, innerlines=()):
+        self.uncoupled = tuple(uncoupled)
+        self.coupled = coupled
+        self.isdual = tuple(bool(x) for x in isdual)
+        self.innerlines = tuple(innerlines)
+        self._h = hash((self.uncoupled, self.coupled, self.isdual, self.innerlines))
+
+    def key(self):
+        return (self.uncoupled, self.coupled, self.isdual, self.innerlines)
+
+    def __eq__(self, o):
+        return isinstance(o, FusionTree) and self.key() == o.key()
+
+    def __hash__(self):
+        return self._h
+
+    def __len__(self):
+        return len(self.uncoupled)
+
+    def __repr__(self):
+        return (f"FusionTree({self.uncoupled}, {self.coupled}, {self.isdual}, "
+                f"{self.innerlines})")
+
+
+def _abelian_inner(uncoupled):
+    """Inner lines of a unique-fusion tree: successive fusion products from the left."""
+    n = len(uncoupled)
+    if n <= 2:
+        return ()
+    inner = []
+    acc = uncoupled[0].otimes(uncoupled[1])[0]
+    inner.append(acc)
+    for k in range(2, n - 1):
+        acc = acc.otimes(uncoupled[k])[0]
+        inner.append(acc)
+    return tuple(inner)
+
+
+def _iter_trees(lists, c):
+    """Yield (uncoupled, innerlines) in the reference iteration order: the last leg's sector
+    varies slowest, then the inner line, then recursively the front legs."""
+    n = len(lists)
+    if n == 0:
+        if c.isunit():
+            yield (), ()
+        return
+    if n == 1:
+        if c in lists[0]:
+            yield (c,), ()
+        return
+    if n == 2:
+        for b in lists[1]:
+            for a in lists[0]:
+                if Nsymbol(a, b, c):
+                    yield (a, b), ()
+        return
+    for b in lists[-1]:
+        for a in c.otimes(b.dual()):
+            for rest_out, rest_lines in _iter_trees(lists[:-1], a):
+                yield rest_out + (b,), rest_lines + (a,)
+
+
+def fusiontrees(uncoupled_lists, coupled, isdual):
+    """All fusion trees with uncoupled sectors drawn from `uncoupled_lists[i]`."""
+    isdual = tuple(bool(x) for x in isdual)
+    return [FusionTree(out, coupled, isdual, lines)
+            for out, lines in _iter_trees(tuple(tuple(l) for l in uncoupled_lists), coupled)]
+
+
+@lru_cache(maxsize=100000)
+def _trees_single(uncoupled, coupled, isdual):
+    return tuple(fusiontrees(tuple((s,) for s in uncoupled), coupled, isdual))
+
+
+class FusionTreeBlock:
+    """All tree pairs (f₁, f₂) sharing the same uncoupled sectors and duality flags."""
+    __slots__ = ("trees", "uncoupled", "isdual", "index", "_h")
+
+    def __init__(self, uncoupled, isdual, unit, trees=None):
+        u1, u2 = tuple(uncoupled[0]), tuple(uncoupled[1])
+        d1, d2 = tuple(bool(x) for x in isdual[0]), tuple(bool(x) for x in isdual[1])
+        self.uncoupled = (u1, u2)
+        self.isdual = (d1, d2)
+        if trees is None:
+            trees = []
+            n1, n2 = len(u1), len(u2)
+            if n1 == 0 and n2 == 0:
+                f = FusionTree((), unit, (), ())
+                trees.append((f, f))
+            else:
+                if n1 == 0:
+                    cs = [c for c in otimes_many(u2, unit) if c.isunit()]
+                elif n2 == 0:
+                    cs = [c for c in otimes_many(u1, unit) if c.isunit()]
+                else:
+                    s2 = set(otimes_many(u2, unit))
+                    cs = [c for c in otimes_many(u1, unit) if c in s2]
+                cs.sort(key=lambda c: c.sortkey())
+                for c in cs:
+                    for f2 in _trees_single(u2, c, d2):
+                        for f1 in _trees_single(u1, c, d1):
+                            trees.append((f1, f2))
+        self.trees = trees
+        self.index = {t: i for i, t in enumerate(trees)}
+        self._h = hash((self.uncoupled, self.isdual))
+
+    def __len__(self):
+        return len(self.trees)
+
+    def __eq__(self, o):
+        return isinstance(o, FusionTreeBlock) and self.trees == o.trees
+
+    def __hash__(self):
+        return self._h
+
+    def numout(self):
+        return len(self.uncoupled[0])
+
+    def numin(self):
+        return len(self.uncoupled[1])
+
+
+def _unit_of(src):
+    f1, f2 = src.trees[0] if isinstance(src, FusionTreeBlock) else src
+    return f1.coupled.unit()
+
+
+# ------------------------------------------------------------------------------------
+# bending (B-moves)
+# ------------------------------------------------------------------------------------
+def _bendright_treepair(f1, f2):
+    n1, n2 = len(f1), len(f2)
+    c = f1.coupled
+    if n1 == 1:
+        a = c.unit()
+    elif n1 == 2:
+        a = f1.uncoupled[0]
+    else:
+        a = f1.innerlines[-1]
+    b = f1.uncoupled[n1 - 1]
+    f1n = FusionTree(f1.uncoupled[:-1], a, f1.isdual[:-1], f1.innerlines[:-1] if n1 > 2 else ())
+    f2n = FusionTree(f2.uncoupled + (b.dual(),), a, f2.isdual + (not f1.isdual[n1 - 1],),
+                     (f2.innerlines + (c,)) if n2 > 1 else ())
+    return (a, b, c), (f1n, f2n)
+
+
+def _bend_coeff(a, b, c, isdual_b):
+    coeff0 = sqrtdim(c) * invsqrtdim(a)
+    if isdual_b:
+        coeff0 = coeff0 * frobenius_schur_phase(b.dual())
+    return coeff0 * Bsymbol(a, b, c)
+
+
+def bendright(src):
+    """Bend the last splitting leg to the fusion side (`duality_manipulations.jl:52-118`)."""
+    if not isinstance(src, FusionTreeBlock):
+        f1, f2 = src
+        (a, b, c), pair = _bendright_treepair(f1, f2)
+        return pair, _bend_coeff(a, b, c, f1.isdual[-1])
+    u1, u2 = src.uncoupled
+    d1, d2 = src.isdual
+    unit = _unit_of(src)
+    dst = FusionTreeBlock((u1[:-1], u2 + (u1[-1].dual(),)), (d1[:-1], d2 + (not d1[-1],)), unit)
+    U = np.zeros((len(dst), len(src)))
+    for col, (f1, f2) in enumerate(src.trees):
+        (a, b, c), pair = _bendright_treepair(f1, f2)
+        U[dst.index[pair], col] = _bend_coeff(a, b, c, f1.isdual[-1])
+    return dst, U
+
+
+def bendleft(src):
+    """Bend the last fusion leg to the splitting side (`duality_manipulations.jl:120-194`)."""
+    if not isinstance(src, FusionTreeBlock):
+        f1, f2 = src
+        (a, b, c), (f2n, f1n) = _bendright_treepair(f2, f1)
+        return (f1n, f2n), _bend_coeff(a, b, c, f2.isdual[-1])  # real: conj is identity
+    u1, u2 = src.uncoupled
+    d1, d2 = src.isdual
+    unit = _unit_of(src)
+    dst = FusionTreeBlock((u1 + (u2[-1].dual(),), u2[:-1]), (d1 + (not d2[-1],), d2[:-1]), unit)
+    U = np.zeros((len(dst), len(src)))
+    for col, (f1, f2) in enumerate(src.trees):
+        (a, b, c), (f2n, f1n) = _bendright_treepair(f2, f1)
+        U[dst.index[(f1n, f2n)], col] = _bend_coeff(a, b, c, f2.isdual[-1])
+    return dst, U
+
+
+def repartition(src, N):
+    """Bend legs until the splitting side has N legs (`duality_manipulations.jl:460-505`)."""
+    if isinstance(src, FusionTreeBlock):
+        n1 = src.numout()
+        n = n1 - N
+        if n == 0:
+            return src, np.eye(len(src))
+        f = bendright if n > 0 else bendleft
+        dst, U = f(src)
+        for _ in range(abs(n) - 1):
+            dst, Ut = f(dst)
+            U = Ut @ U
+        return dst, U
+    f1, f2 = src
+    n = len(f1) - N
+    if n == 0:
+        return src, 1.0
+    f = bendright if n > 0 else bendleft
+    dst, coeff = f(src)
+    for _ in range(abs(n) - 1):
+        dst, ct = f(dst)
+        coeff = ct * coeff
+    return dst, coeff
+
+
+# ------------------------------------------------------------------------------------
+# braiding
+# ------------------------------------------------------------------------------------
+def linearizepermutation(p1, p2, n1, n2):
+    """1-based linearisation of (p₁, p₂) onto a single splitting tree (`auxiliary.jl:1-11`)."""
+    q1 = tuple((n2 + 2 * n1 + 1 - x) if x > n1 else x for x in p1)
+    q2 = tuple((n2 + 2 * n1 + 1 - x) if x > n1 else x for x in reversed(p2))
+    return q1 + q2
+
+
+def permutation2swaps(perm):
+    """Bubble decomposition of a 1-based permutation into adjacent swaps (`auxiliary.jl:13-28`)."""
+    p = list(perm)
+    N = len(p)
+    swaps = []
+    for k in range(1, N):
+        swaps.extend(range(p[k - 1] - 1, k - 1, -1))
+        for l in range(k + 1, N + 1):
+            if p[l - 1] < p[k - 1]:
+                p[l - 1] += 1
+        p[k - 1] = k
+    return swaps
+
+
+def _artin_braid_block(src, i, inv):
+    """Elementary braid of legs i, i+1 (1-based) on a block with N₂ = 0."""
+    u = src.uncoupled[0]
+    N = len(u)
+    if not 1 <= i < N:
+        raise ValueError(f"Cannot swap outputs i={i} and i+1 out of only {N} outputs")
+    dflag = src.isdual[0]
+    a, b = u[i - 1], u[i]
+    un = list(u)
+    un[i - 1], un[i] = b, a
+    un = tuple(un)
+    dn = list(dflag)
+    dn[i - 1], dn[i] = dflag[i], dflag[i - 1]
+    dn = tuple(dn)
+    unit = _unit_of(src)
+    coupled_n = unit
+    dst = FusionTreeBlock((un, ()), (dn, ()), unit)
+    U = np.zeros((len(dst), len(src)))
+    if a.isunit() or b.isunit():
+        for col, (f, f2) in enumerate(src.trees):
+            inner = f.innerlines
+            ext = (u[0],) + inner + (coupled_n,)
+            innern = inner
+            if i > 1:
+                innern = list(inner)
+                innern[i - 2] = ext[i] if a.isunit() else ext[i - 2]
+                innern = tuple(innern)
+            fn = FusionTree(un, coupled_n, dn, innern)
+            U[dst.index[(fn, f2)], col] = 1.0
+        return dst, U
+    for col, (f, f2) in enumerate(src.trees):
+        inner = f.innerlines
+        ext = (u[0],) + inner + (coupled_n,)
+        if i == 1:
+            c = inner[0] if N > 2 else coupled_n
+            R = Rsymbol(b, a, c) if inv else Rsymbol(a, b, c)
+            fn = FusionTree(un, coupled_n, dn, inner)
+            U[dst.index[(fn, f2)], col] = R
+            continue
+        bb, dd = u[i - 1], u[i]
+        aa, cc, ee = ext[i - 2], ext[i - 1], ext[i]
+        s2 = set(ee.otimes(bb.dual()))
+        for cp in aa.otimes(dd):
+            if cp not in s2:
+                continue
+            if inv:
+                coeff = (Rsymbol(dd, cc, ee) * Fsymbol(dd, aa, bb, ee, cp, cc)) * Rsymbol(dd, aa, cp)
+            else:
+                coeff = Rsymbol(cc, dd, ee) * (Fsymbol(dd, aa, bb, ee, cp, cc) * Rsymbol(aa, dd, cp))
+            if coeff == 0:
+                continue
+            innern = list(inner)
+            innern[i - 2] = cp
+            fn = FusionTree(un, coupled_n, dn, tuple(innern))
+            U[dst.index[(fn, f2)], col] = coeff
+    return dst, U
+
+
+def artin_braid(src, i, inv=False):
+    if isinstance(src, FusionTreeBlock):
+        return _artin_braid_block(src, i, inv)
+    raise NotImplementedError("single-tree artin_braid is only used through braid()")
+
+
+def _braid_unique_tree(f, p):
+    """Braid of a unique-fusion splitting tree with symmetric braiding: coefficient is the
+    product of R-symbols of every crossing pair (`braiding_manipulations.jl:226-242`)."""
+    N = len(f)
+    coeff = 1.0
+    for i in range(N):
+        for j in range(i):
+            if p[j] > p[i]:
+                a, b = f.uncoupled[p[j] - 1], f.uncoupled[p[i] - 1]
+                coeff = coeff * Rsymbol(a, b, a.otimes(b)[0])
+    un = tuple(f.uncoupled[k - 1] for k in p)
+    dn = tuple(f.isdual[k - 1] for k in p)
+    return FusionTree(un, f.coupled, dn, _abelian_inner(un)), coeff
+
+
+def _fsbraid_pair(pair, p1, p2, l1, l2):
+    f1, f2 = pair
+    n1s, n2s = len(f1), len(f2)
+    p = linearizepermutation(p1, p2, n1s, n2s)
+    (f, f0), coeff1 = repartition((f1, f2), n1s + n2s)
+    fp, coeff2 = _braid_unique_tree(f, p)
+    (g1, g2), coeff3 = repartition((fp, f0), len(p1))
+    return (g1, g2), coeff1 * coeff2 * coeff3
+
+
+def _fsbraid_block(src, p1, p2, l1, l2):
+    N1 = len(p1)
+    N2 = len(p2)
+    p = linearizepermutation(p1, p2, src.numout(), src.numin())
+    levels = list(l1) + list(reversed(l2))
+    dst, U = repartition(src, src.numout() + src.numin())
+    for s in permutation2swaps(p):
+        inv = levels[s - 1] > levels[s]
+        dst, Ut = _artin_braid_block(dst, s, inv)
+        U = Ut @ U
+        levels[s - 1], levels[s] = levels[s], levels[s - 1]
+    if N2 == 0:
+        return dst, U
+    dst, Ut = repartition(dst, N1)
+    U = Ut @ U
+    return dst, U
+
+
+_FSBRAID_CACHE: dict = {}
+
+
+def braid(src, p, levels):
+    """Braid a tree pair (unique fusion) or a FusionTreeBlock; p = (p₁, p₂) 1-based,
+    levels = (levels₁, levels₂)."""
+    p1, p2 = tuple(p[0]), tuple(p[1])
+    l1, l2 = tuple(levels[0]), tuple(levels[1])
+    if isinstance(src, FusionTreeBlock):
+        key = (src.uncoupled, src.isdual, p1, p2, l1, l2)
+        hit = _FSBRAID_CACHE.get(key)
+        if hit is None:
+            hit = _fsbraid_block(src, p1, p2, l1, l2)
+            if len(_FSBRAID_CACHE) > 10000:
+                _FSBRAID_CACHE.clear()
+            _FSBRAID_CACHE[key] = hit
+        return hit
+    return _fsbraid_pair(src, p1, p2, l1, l2)
+
+
+def permute(src, p):
+    """Permute = braid with levels 1..N (`braiding_manipulations.jl:356-361`)."""
+    if isinstance(src, FusionTreeBlock):
+        n1, n2 = src.numout(), src.numin()
+    else:
+        n1, n2 = len(src[0]), len(src[1])
+    l1 = tuple(range(1, n1 + 1))
+    l2 = tuple(range(n1 + 1, n1 + n2 + 1))
+    return braid(src, p, (l1, l2))

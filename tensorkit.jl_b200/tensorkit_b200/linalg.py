@@ -1,0 +1,181 @@
+"""Blockwise linear algebra on device tensors: mul!, norm, tr, inner/dot, scale!, add!.
+
+Follows `src/tensors/linalg.jl`:
+- `mul!(tC, tA, tB, α, β)` (`:330-370`): merge over the sorted coupled sectors; every sector
+  present in A, B and C gets C_c = α·A_c·B_c + β·C_c, a sector of C missing from A or B gets
+  C_c = β·C_c. All blocks go to one grouped launch (libtkb200 `tkb_grouped_gemm`), in
+  plain FP64 or split precision (`backend.set_precision`).
+- `norm` (`:257-282`) = sqrt(Σ_c dim(c)·‖B_c‖²); `tr` (`:319-327`) = Σ_c dim(c)·tr(B_c);
+  `inner` (`src/tensors/vectorinterface.jl:114-130`) = Σ_c dim(c)·⟨X_c, Y_c⟩.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+
+from . import _lib as L
+from .backend import GemmPlan, ReducePlan, get_context, precision
+from .indexmanipulations import _check_device, _scalar, _sync_in, _sync_out, dtype_code, permute_
+from .spaces import SpaceMismatch
+from .structure import blockstructure
+from .tensor import AdjointTensorMap, TensorMap
+
+__all__ = ["mul_", "compose", "norm", "tr", "inner", "dot", "scale_", "add_", "gemm_plan",
+           "block_gemm_descriptors"]
+
+
+def _operand_blocks(t):
+    """{c: (offset, rows, cols, ld, op)} for op(block) of a TensorMap or lazy adjoint."""
+    out = {}
+    if isinstance(t, AdjointTensorMap):
+        bs = blockstructure(t.parent.space)
+        op = L.TKB_OP_C if t.is_complex() else L.TKB_OP_T
+        for c, ((d1, d2), (a, _)) in bs.items():
+            out[c] = (a, d2, d1, d1, op)
+        return out
+    for c, ((d1, d2), (a, _)) in blockstructure(t.space).items():
+        out[c] = (a, d1, d2, d1, L.TKB_OP_N)
+    return out
+
+
+def block_gemm_descriptors(tC, tA, tB):
+    """Per-block (m, n, k, offA, offB, offC, lda, ldb, ldc, opA, opB) in C's sector order."""
+    A = _operand_blocks(tA)
+    B = _operand_blocks(tB)
+    out = []
+    for c, ((d1, d2), (offc, _)) in blockstructure(tC.space).items():
+        if c in A and c in B:
+            oa, ma, ka, lda, opa = A[c]
+            ob, kb, nb, ldb, opb = B[c]
+            assert ma == d1 and nb == d2 and ka == kb
+            out.append((d1, d2, ka, oa, ob, offc, lda, ldb, d1, opa, opb))
+        else:
+            out.append((d1, d2, 0, 0, 0, offc, 1, 1, d1, L.TKB_OP_N, L.TKB_OP_N))
+    return out
+
+
+def _spacekey(t):
+    if isinstance(t, AdjointTensorMap):
+        return ("adj", t.parent.space)
+    return ("map", t.space)
+
+
+def gemm_plan(ctx, tC, tA, tB, prec=None, slices=None):
+    mode, sl = precision()
+    if prec is not None:
+        mode = prec
+    if slices is not None:
+        sl = slices
+    code = dtype_code(tC.data)
+    key = ("gemm", tC.space, _spacekey(tA), _spacekey(tB), code, mode, sl)
+
+    def make():
+        blocks = block_gemm_descriptors(tC, tA, tB)
+        lens = (tA.data.numel(), tB.data.numel(), tC.data.numel())
+        return GemmPlan(ctx, blocks, lens, code,
+                        L.TKB_SPLIT_INT8 if mode == "split" else L.TKB_PLAIN, sl)
+
+    return ctx.plans.get_or(key, make)
+
+
+def mul_(tC: TensorMap, tA, tB, alpha=1.0, beta=0.0, prec=None, slices=None):
+    """tC = α·tA·tB + β·tC, blockwise over coupled sectors."""
+    if tA.space.compose(tB.space) != tC.space:
+        raise SpaceMismatch(f"{tC.space} ≠ {tA.space} * {tB.space}")
+    _check_device(tC, tA, tB)
+    if not (tA.data.dtype == tB.data.dtype == tC.data.dtype):
+        raise TypeError("mul! operands must share their scalar type")
+    ctx = get_context(tC.data.device.index)
+    plan = gemm_plan(ctx, tC, tA, tB, prec, slices)
+    _sync_in(ctx)
+    L.check(ctx.lib.tkb_grouped_gemm(ctx.handle, plan.handle, C.c_void_p(tC.data.data_ptr()),
+                                     C.c_void_p(tA.data.data_ptr()), C.c_void_p(tB.data.data_ptr()),
+                                     _scalar(alpha), _scalar(beta)), ctx.handle)
+    _sync_out(ctx, tC)
+    return tC
+
+
+def compose(tA, tB):
+    """tA * tB as a new tensor (TensorKit's `*` on tensor maps)."""
+    import torch
+    W = tA.space.compose(tB.space)
+    tC = TensorMap(torch.empty(W.dim(), dtype=tA.data.dtype, device=tA.data.device), W)
+    return mul_(tC, tA, tB, 1.0, 0.0)
+
+
+def _rplan(ctx, key, segs, length):
+    return ctx.rplans.get_or(key, lambda: ReducePlan(ctx, segs, length))
+
+
+def _reduce(ctx, plan, kind, x, y=None):
+    import numpy as np
+    out = np.zeros(2)
+    _sync_in(ctx)
+    L.check(ctx.lib.tkb_reduce(ctx.handle, plan.handle, kind, dtype_code(x),
+                               C.c_void_p(x.data_ptr()), C.c_void_p(y.data_ptr() if y is not None else 0),
+                               out.ctypes.data_as(C.POINTER(C.c_double))), ctx.handle)
+    return out
+
+
+def _block_segments(W):
+    return [(a, d1 * d2, 1, float(c.dim())) for c, ((d1, d2), (a, _)) in blockstructure(W).items()]
+
+
+def _tensor_data_space(t):
+    if isinstance(t, AdjointTensorMap):
+        return t.parent.data, t.parent.space, True
+    return t.data, t.space, False
+
+
+def norm(t) -> float:
+    data, W, _ = _tensor_data_space(t)
+    _check_device(t)
+    ctx = get_context(data.device.index)
+    plan = _rplan(ctx, ("norm", W), _block_segments(W), data.numel())
+    r = _reduce(ctx, plan, L.TKB_NORM2, data)
+    return math.sqrt(max(r[0], 0.0))
+
+
+def inner(tx, ty):
+    """Σ_c dim(c)·⟨X_c, Y_c⟩ (conjugate-linear in the first argument)."""
+    if tx.space != ty.space:
+        raise SpaceMismatch(f"{tx.space} ≠ {ty.space}")
+    if isinstance(tx, AdjointTensorMap) or isinstance(ty, AdjointTensorMap):
+        raise NotImplementedError("inner of lazy adjoints: materialise with permute first")
+    _check_device(tx, ty)
+    ctx = get_context(tx.data.device.index)
+    plan = _rplan(ctx, ("norm", tx.space), _block_segments(tx.space), tx.data.numel())
+    r = _reduce(ctx, plan, L.TKB_INNER, tx.data, ty.data)
+    return complex(r[0], r[1]) if tx.is_complex() else float(r[0])
+
+
+dot = inner
+
+
+def tr(t):
+    if t.space.domain != t.space.codomain:
+        raise SpaceMismatch("Trace of a tensor only exist when domain == codomain")
+    data, W, isadj = _tensor_data_space(t)
+    _check_device(t)
+    ctx = get_context(data.device.index)
+    segs = [(a, d1, d1 + 1, float(c.dim())) for c, ((d1, d2), (a, _)) in blockstructure(W).items()]
+    plan = _rplan(ctx, ("tr", W), segs, data.numel())
+    r = _reduce(ctx, plan, L.TKB_TRACE, data)
+    if data.is_complex():
+        v = complex(r[0], r[1])
+        return v.conjugate() if isadj else v
+    return float(r[0])
+
+
+def scale_(t: TensorMap, alpha):
+    """t = α·t: an identity-permutation transform of a copy with β = 0."""
+    tmp = TensorMap(t.data.clone(), t.space)
+    return add_(t, tmp, alpha, 0.0)
+
+
+def add_(ty: TensorMap, tx, alpha=1.0, beta=1.0):
+    """ty = β·ty + α·tx (TensorKit add!, src/tensors/vectorinterface.jl:93-99)."""
+    if ty.space != tx.space:
+        raise SpaceMismatch(f"{ty.space} ≠ {tx.space}")
+    p = (tx.codomainind(), tx.domainind())
+    return permute_(ty, tx, p, alpha, beta)
