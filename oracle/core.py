@@ -523,7 +523,12 @@ def braid_pair(pair, p1, p2, l1, l2):
                     new[(tn, t0)] = new.get((tn, t0), 0.0) + y * x
             lc = new
             levels[s - 1], levels[s] = levels[s], levels[s - 1]
-    return repartition(lc, len(p1))
+    # the final repartition is composed on its own and then applied (U = U_tmp * U)
+    out = {}
+    for pr, x in lc.items():
+        for q, y in repartition({pr: 1.0}, len(p1)).items():
+            out[q] = out.get(q, 0.0) + y * x
+    return out
 
 
 def permute_pair(pair, p):

@@ -21,7 +21,7 @@ import ctypes as C
 from . import _lib as L
 from .backend import DeviceTable, get_context
 from .spaces import SpaceMismatch
-from .tensor import AdjointTensorMap, TensorMap
+from .tensor import AdjointTensorMap, TensorMap, new_tensor
 from .treetransformers import flatten_transformer, treebraider
 
 __all__ = ["permute", "permute_", "braid", "braid_", "add_transform_", "transpose",
@@ -126,9 +126,7 @@ def permute(t, p, copy=False):
         if (tuple(map(adj, p[1])), tuple(map(adj, p[0]))) == (t.parent.codomainind(),
                                                                t.parent.domainind()):
             return t
-    import torch
-    dst = TensorMap(torch.empty(t.space.permute(p).dim(), dtype=t.data.dtype, device=t.data.device),
-                    t.space.permute(p))
+    dst = new_tensor(t.space.permute(p), t.data.dtype, t.data.device)
     return permute_(dst, t, p, 1.0, 0.0)
 
 
@@ -136,9 +134,7 @@ def braid(t, p, levels, copy=False):
     p = _norm_p(p)
     if not copy and isinstance(t, TensorMap) and p == (t.codomainind(), t.domainind()):
         return t
-    import torch
-    W = t.space.permute(p)
-    dst = TensorMap(torch.empty(W.dim(), dtype=t.data.dtype, device=t.data.device), W)
+    dst = new_tensor(t.space.permute(p), t.data.dtype, t.data.device)
     return braid_(dst, t, p, levels, 1.0, 0.0)
 
 
@@ -157,9 +153,7 @@ def transpose(t, p=None, copy=False):
     if p is None:
         p = (tuple(reversed(t.domainind())), tuple(reversed(t.codomainind())))
     p = _norm_p(p)
-    import torch
-    W = t.space.permute(p)
-    dst = TensorMap(torch.empty(W.dim(), dtype=t.data.dtype, device=t.data.device), W)
+    dst = new_tensor(t.space.permute(p), t.data.dtype, t.data.device)
     return transpose_(dst, t, p)
 
 

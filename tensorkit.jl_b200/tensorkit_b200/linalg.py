@@ -18,7 +18,7 @@ from .backend import GemmPlan, ReducePlan, get_context, precision
 from .indexmanipulations import _check_device, _scalar, _sync_in, _sync_out, dtype_code, permute_
 from .spaces import SpaceMismatch
 from .structure import blockstructure
-from .tensor import AdjointTensorMap, TensorMap
+from .tensor import AdjointTensorMap, TensorMap, new_tensor
 
 __all__ = ["mul_", "compose", "norm", "tr", "inner", "dot", "scale_", "add_", "gemm_plan",
            "block_gemm_descriptors"]
@@ -97,9 +97,8 @@ def mul_(tC: TensorMap, tA, tB, alpha=1.0, beta=0.0, prec=None, slices=None):
 
 def compose(tA, tB):
     """tA * tB as a new tensor (TensorKit's `*` on tensor maps)."""
-    import torch
     W = tA.space.compose(tB.space)
-    tC = TensorMap(torch.empty(W.dim(), dtype=tA.data.dtype, device=tA.data.device), W)
+    tC = new_tensor(W, tA.data.dtype, tA.data.device)
     return mul_(tC, tA, tB, 1.0, 0.0)
 
 

@@ -19,12 +19,26 @@ import numpy as np
 from .spaces import HomSpace, SpaceMismatch
 from .structure import blockstructure, degeneracystructure, sectorstructure, subblockstructure
 
-__all__ = ["TensorMap", "AdjointTensorMap", "randn_tensor", "zeros_tensor", "space_randn_data"]
+__all__ = ["TensorMap", "AdjointTensorMap", "randn_tensor", "zeros_tensor", "space_randn_data",
+           "new_tensor"]
 
 
 def _torch():
     import torch
     return torch
+
+
+# While a CUDA graph is being captured every buffer allocated for the network must outlive
+# the capture (the graph replays into those addresses); allocations are logged here.
+_ALLOC_LOG: list | None = None
+
+
+def new_tensor(W: HomSpace, dtype, device) -> "TensorMap":
+    torch = _torch()
+    t = TensorMap(torch.empty(W.dim(), dtype=dtype, device=device), W)
+    if _ALLOC_LOG is not None:
+        _ALLOC_LOG.append(t.data)
+    return t
 
 
 def space_randn_data(W: HomSpace, seed: int, dtype="float64") -> np.ndarray:

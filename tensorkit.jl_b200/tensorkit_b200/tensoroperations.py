@@ -24,7 +24,7 @@ import re
 from .indexmanipulations import permute, permute_
 from .linalg import mul_
 from .spaces import HomSpace, SpaceMismatch
-from .tensor import AdjointTensorMap, TensorMap
+from .tensor import AdjointTensorMap, TensorMap, new_tensor
 
 __all__ = ["tensoradd_", "tensorcontract_", "tensorcontract", "contract_", "blas_contract_",
            "tensoradd_structure", "tensorcontract_structure", "tensor", "parse_tensor_expr",
@@ -152,8 +152,7 @@ def contract_(C, A, pA, B, pB, pAB, alpha=1.0, beta=0.0):
 
 
 def _alloc(W, like):
-    import torch
-    return TensorMap(torch.empty(W.dim(), dtype=like.data.dtype, device=like.data.device), W)
+    return new_tensor(W, like.data.dtype, like.data.device)
 
 
 def blas_contract_(C, A, pA, B, pB, pAB, alpha=1.0, beta=0.0, plan_hook=None):

@@ -1,0 +1,77 @@
+"""Parity of the grouped block GEMM (mul!) with the oracle, plain FP64 and split precision.
+
+Mirrors mul! semantics (src/tensors/linalg.jl:330-370): matching coupled sectors multiply,
+sectors of C missing from A or B are scaled by β. Tolerances: plain FP64 1e-12 relative
+(max-norm over the result); split precision (int8 slices) 1e-12 relative at the default
+7 slices."""
+import numpy as np
+import pytest
+
+from helpers import O, VSU2, cfg1_spaces, cfg2_spaces, relerr, to_device, to_hom
+import tensorkit_b200 as tk
+
+pytestmark = pytest.mark.gpu
+TOL_PLAIN = 1e-12
+TOL_SPLIT = 1e-12
+
+
+def _mats(cplx, mult=1):
+    V, Pp = cfg2_spaces(mult)
+    WA = O.Hom([V, Pp], [V])
+    WB = O.Hom([V], [V])
+    A = O.randn(WA, 1, cplx)
+    B = O.randn(WB, 2, cplx)
+    return A, B
+
+
+@pytest.mark.parametrize("prec", ["plain", "split"])
+@pytest.mark.parametrize("cplx", [False, True])
+def test_mul_su2(prec, cplx):
+    A, B = _mats(cplx)
+    ref = O.mul(A, B)
+    Ad, Bd = to_device(A), to_device(B)
+    C = tk.TensorMap.zeros(to_hom(ref.W), dtype=Ad.dtype, device=Ad.device)
+    tk.mul_(C, Ad, Bd, 1.0, 0.0, prec=prec)
+    assert relerr(C.to_host(), ref.data) <= (TOL_PLAIN if prec == "plain" else TOL_SPLIT)
+
+
+@pytest.mark.parametrize("prec", ["plain", "split"])
+def test_mul_alpha_beta_adjoint(prec):
+    A, B = _mats(True)
+    # C = α·A'·A + β·C with a lazy adjoint left operand
+    ref0 = O.mul(A, A, adjA=True)
+    C0 = O.randn(ref0.W, 9, True)
+    Ad = to_device(A)
+    Cd = to_device(C0)
+    alpha, beta = 0.75 + 0.5j, -1.5 + 0.25j
+    tk.mul_(Cd, tk.AdjointTensorMap(Ad), Ad, alpha, beta, prec=prec)
+    ref = alpha * ref0.data + beta * C0.data
+    assert relerr(Cd.to_host(), ref) <= (TOL_PLAIN if prec == "plain" else TOL_SPLIT)
+
+
+@pytest.mark.parametrize("prec", ["plain", "split"])
+def test_mul_missing_sectors_scale_by_beta(prec):
+    """Sectors of C absent from A·B get C_c = β·C_c."""
+    V = O.Space({O.U1(q): 3 for q in range(-2, 3)})
+    V2 = O.Space({O.U1(q): 2 for q in range(0, 2)})
+    WA = O.Hom([V], [V2])
+    WB = O.Hom([V2], [V])
+    A, B = O.randn(WA, 1), O.randn(WB, 2)
+    ref = O.mul(A, B)
+    C0 = O.randn(ref.W, 3)
+    Cd = to_device(C0)
+    tk.mul_(Cd, to_device(A), to_device(B), 2.0, 0.5, prec=prec)
+    want = 2.0 * ref.data + 0.5 * C0.data
+    assert relerr(Cd.to_host(), want) <= 1e-12
+
+
+@pytest.mark.parametrize("slices", [4, 5, 6, 7])
+def test_split_error_decreases_with_slices(slices):
+    A, B = _mats(False)
+    ref = O.mul(A, B)
+    Ad, Bd = to_device(A), to_device(B)
+    C = tk.TensorMap.zeros(to_hom(ref.W), device=Ad.device)
+    tk.mul_(C, Ad, Bd, prec="split", slices=slices)
+    err = relerr(C.to_host(), ref.data)
+    # truncation bound of the slicing: ~2^-7S per operand, times a modest k-dependent factor
+    assert err <= 2.0 ** (-7 * slices) * 64
