@@ -1,0 +1,431 @@
+"""Benchmark: GFLOP/s of the symmetric contraction path on B200.
+
+Default workload (one GPU): the large SU(2) environment update
+    En[a;b] := conj(A[c,p;a]) * E[c;d] * A[d,p;b]
+with V = SU(2) spins 0..3 (step 1/2), degeneracies {32,48,40,24,12,6,2}×8 (dim 3632),
+P = spin 1/2; Float64, seeded synthetic data. A step is one whole contraction (two
+pairwise tensorcontract! = 4 transforms + 2 grouped GEMMs), replayed as a CUDA graph.
+`value` is the split-precision (int8 tensor-core slices, FP64 recombination) GFLOP/s,
+`plain_fp64` the plain FP64 (DMMA) GFLOP/s of the same step. L2 (126 MB) is flushed
+between timed steps by writing a 256 MB buffer outside the timed events.
+
+Usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                       [--workload su2_large|u1_heff|su2_env|u1_small] [--breakdown]
+Multi-GPU (torchrun, one process per GPU): replicas only — every rank runs its own
+contractions, the step time is the max over ranks, `value` the total over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+for _p in (ROOT, os.path.join(ROOT, "tensorkit.jl_b200"), os.path.join(ROOT, "tests")):
+    if _p not in sys.path:
+        sys.path.insert(0, _p)
+
+METRIC = "U1/SU2 contract GFLOP/s: split-prec TC vs plain FP64, 1 B200, <=1e-12 rel err"
+
+WORKLOADS = {
+    "su2_large": dict(expr="En[a;b] := conj(A[c,p;a])*E[c;d]*A[d,p;b]",
+                      desc="SU(2) environment update, V dim 3632 (degeneracies x8), P = 1/2, Float64"),
+    "su2_env": dict(expr="En[a;b] := conj(A[c,p;a])*E[c;d]*A[d,p;b]",
+                    desc="SU(2) environment update, V dim 454, P = 1/2, Float64"),
+    "u1_heff": dict(expr="y[a,p,q;b] := L[a,w;c]*x[c,r,s;d]*W1[w,p;r,v]*W2[v,q;s,u]*R[d,u;b]",
+                    desc="U(1) two-site effective Hamiltonian, V dim 1924, W = {-1:2,0:3,1:2}, Float64"),
+    "u1_small": dict(expr="C[a,p,q;b] := A[a,p;c]*B[c,q;b]",
+                     desc="U(1) small, V dim 56, P = {-1,0,1}, Float64"),
+}
+
+
+def oracle_inputs(name):
+    from helpers import O, cfg1_spaces, cfg2_spaces, cfg3_spaces
+    if name in ("su2_large", "su2_env"):
+        V, Pp = cfg2_spaces(8 if name == "su2_large" else 1)
+        seed = 3 if name == "su2_large" else 1
+        return {"A": O.randn(O.Hom([V, Pp], [V]), seed), "E": O.randn(O.Hom([V], [V]), seed)}
+    if name == "u1_heff":
+        V, Pp, Wm = cfg3_spaces()
+        Wd = Wm.flipdual()
+        return {"L": O.randn(O.Hom([V, Wd], [V]), 2), "x": O.randn(O.Hom([V, Pp, Pp], [V]), 2),
+                "W1": O.randn(O.Hom([Wm, Pp], [Pp, Wm]), 2), "W2": O.randn(O.Hom([Wm, Pp], [Pp, Wm]), 2),
+                "R": O.randn(O.Hom([V, Wm], [V]), 2)}
+    V, Pp = cfg1_spaces()
+    W = O.Hom([V, Pp], [V])
+    return {"A": O.randn(W, 0), "B": O.randn(W, 0)}
+
+
+def oracle_eval(name, tensors):
+    from oracle import core as O
+    from tensorkit_b200.tensoroperations import parse_tensor_expr
+    _, lhs, _, factors = parse_tensor_expr(WORKLOADS[name]["expr"])
+    return O.network(factors, lhs, tensors)
+
+
+# ---- clocks ------------------------------------------------------------------------------
+class ClockSampler:
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.QUERY}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ---- reference arm (CPU) -------------------------------------------------------------------
+def run_reference(args):
+    """The reference's path on the host cores: the oracle restatement of TensorKit's CPU
+    algorithm (Julia is not available), numpy/BLAS with every host thread."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    tens = oracle_inputs(args.workload)
+    oracle_eval(args.workload, tens)  # warm caches (symbols, layouts)
+    flops = workload_flops(args.workload)
+    times = []
+    for i in range(args.warmup + args.steps):
+        t0 = time.perf_counter()
+        oracle_eval(args.workload, tens)
+        dt = time.perf_counter() - t0
+        if i >= args.warmup:
+            times.append(dt)
+    tot = sum(times)
+    v = flops * len(times) / tot / 1e9
+    cores = os.cpu_count()
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "GFLOP/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * tot / len(times),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded PCG64 normals)",
+            "config": {"workload": args.workload, "desc": WORKLOADS[args.workload]["desc"]},
+            "cpu_baseline": {"value": v, "unit": "GFLOP/s", "cores": cores, "kind": "port",
+                             "sample": f"{args.steps} full contractions, numpy/BLAS on {cores} host threads"},
+            "e2e": {"value": v, "unit": "GFLOP/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+    return 0
+
+
+_FLOPS = {}
+
+
+def workload_flops(name):
+    """Algorithmic flops (Σ 2mnk over the block GEMMs) of one step, from the host plans."""
+    if name in _FLOPS:
+        return _FLOPS[name]
+    from oracle import core as O
+    from tensorkit_b200.tensoroperations import parse_tensor_expr
+    tens = oracle_inputs(name)
+    _, lhs, _, factors = parse_tensor_expr(WORKLOADS[name]["expr"])
+    # count on the oracle's pairwise GEMMs: instrument O.mul
+    total = [0.0]
+    orig = O.mul
+
+    def counting(A, B, adjA=False, adjB=False):
+        C = orig(A, B, adjA, adjB)
+        WA = A.W.adjoint() if adjA else A.W
+        bA = O.layout(WA)
+        for c, (d1, d2, _) in O.layout(C.W)[1].items():
+            if c in bA[1]:
+                k = bA[1][c][1]
+                total[0] += 2.0 * d1 * d2 * k * (4 if C.data.dtype.kind == "c" else 1)
+        return C
+    O.mul = counting
+    try:
+        O.network(factors, lhs, tens)
+    finally:
+        O.mul = orig
+    _FLOPS[name] = total[0]
+    return total[0]
+
+
+# ---- our arm -------------------------------------------------------------------------------
+def run_ours(args):
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120))
+
+    import tensorkit_b200 as tk
+    from helpers import to_device
+    from tensorkit_b200 import linalg as LA
+
+    dev = torch.device("cuda", local)
+    tens_o = oracle_inputs(args.workload)
+    inputs = {k: to_device(v, dev) for k, v in tens_o.items()}
+    expr = WORKLOADS[args.workload]["expr"]
+    ctx = tk.get_context(local)
+    stream = ctx.stream
+
+    from tensorkit_b200 import indexmanipulations as IM
+    plans = {}
+    logs = {}
+    for prec in ("split", "plain"):
+        p = tk.NetworkPlan(expr, precision=prec, **inputs)
+        IM.LAUNCH_LOG = []
+        p.run_eager()
+        logs[prec] = IM.LAUNCH_LOG
+        IM.LAUNCH_LOG = None
+        plans[prec] = p.capture()
+    flops = sum(e[1].flops for e in logs["plain"] if e[0] == "gemm")
+
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+
+    def timed(plan, steps, warm):
+        with torch.cuda.stream(stream):
+            for _ in range(warm):
+                plan.replay()
+            stream.synchronize()
+            if world > 1:
+                dist.barrier()
+            evs = []
+            for _ in range(steps):
+                flush.zero_()
+                a = torch.cuda.Event(enable_timing=True)
+                b = torch.cuda.Event(enable_timing=True)
+                a.record(stream)
+                plan.replay()
+                b.record(stream)
+                evs.append((a, b))
+            stream.synchronize()
+            ms = sum(a.elapsed_time(b) for a, b in evs)
+        t = torch.tensor([ms], dtype=torch.float64, device=dev)
+        if world > 1:
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    with ClockSampler(local) as clk:
+        ms_split = timed(plans["split"], args.steps, args.warmup)
+        ms_plain = timed(plans["plain"], args.steps, args.warmup)
+    clocks = clk.summary()
+
+    # precision of this run's outputs vs the oracle (rank 0 computes the oracle once)
+    ref = oracle_eval(args.workload, tens_o).data if rank == 0 else None
+    out_split = plans["split"].output.to_host()
+    out_plain = plans["plain"].output.to_host()
+    err = {}
+    if ref is not None:
+        den = np.abs(ref).max()
+        err = {"split": float(np.abs(out_split - ref).max() / den),
+               "plain": float(np.abs(out_plain - ref).max() / den)}
+
+    # end to end through the public API: pinned host inputs -> device, graph, result -> host
+    host_in = {k: torch.from_numpy(np.ascontiguousarray(v.data)).pin_memory() for k, v in tens_o.items()}
+    host_out = torch.empty(plans["split"].output.data.numel(), dtype=torch.float64).pin_memory()
+    h2d = sum(v.numel() * v.element_size() for v in host_in.values())
+    d2h = host_out.numel() * host_out.element_size()
+
+    def e2e_step(plan):
+        for k, v in host_in.items():
+            plan.inputs[k].data.copy_(v, non_blocking=True)
+        plan.replay()
+        host_out.copy_(plan.output.data, non_blocking=True)
+
+    with torch.cuda.stream(stream):
+        for _ in range(args.warmup):
+            e2e_step(plans["split"])
+        stream.synchronize()
+        if world > 1:
+            dist.barrier()
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        for _ in range(args.steps):
+            e2e_step(plans["split"])
+        b.record(stream)
+        stream.synchronize()
+        ms_e2e = a.elapsed_time(b)
+    te = torch.tensor([ms_e2e], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(te, op=dist.ReduceOp.MAX)
+    ms_e2e = float(te.item())
+
+    # per-kernel breakdown of one split step; the dominant kernel gives the roofline entry
+    roof, breakdown = kernel_roofline(args, logs["split"], ctx, flush) if rank == 0 else (None, None)
+
+    value = flops * world * args.steps / (ms_split * 1e-3) / 1e9
+    plain_value = flops * world * args.steps / (ms_plain * 1e-3) / 1e9
+    e2e_value = flops * world * args.steps / (ms_e2e * 1e-3) / 1e9
+    line = None
+    if rank == 0:
+        cpu = cpu_baseline(args, tens_o, flops) if world == 1 else None
+        line = {"metric": METRIC, "value": value, "unit": "GFLOP/s", "n_gpus": world,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_split / args.steps,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                "data": "synthetic (seeded PCG64 normals)",
+                "config": {"workload": args.workload, "desc": WORKLOADS[args.workload]["desc"],
+                           "expr": expr, "flops_per_step": flops, "l2": "flushed (256 MB write) between steps",
+                           "parallelism": f"replicas x{world}", "graph": "CUDA graph per step"},
+                "plain_fp64": {"value": plain_value, "unit": "GFLOP/s", "ms_per_step": ms_plain / args.steps},
+                "split_over_plain": value / plain_value,
+                "max_rel_err": err,
+                "e2e": {"value": e2e_value, "unit": "GFLOP/s", "h2d_bytes_per_step": h2d,
+                        "d2h_bytes_per_step": d2h, "ms_per_step": ms_e2e / args.steps},
+                "gpu_launches": (plans["split"].kernels_per_replay) * args.steps,
+                "roofline": roof, "breakdown": breakdown, "cpu_baseline": cpu, "clocks": clocks}
+        print(json.dumps(line))
+    for p in plans.values():
+        p.free()
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def kernel_roofline(args, log, ctx, flush):
+    """Re-time every launch of one step alone (CUDA events on the library stream, L2 flushed
+    before each) and relate the dominant kernel's algorithmic work to the measured peak."""
+    import torch
+    from tensorkit_b200.indexmanipulations import relaunch
+
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+        src = "measured"
+    except Exception:
+        peaks, src = {}, "fallback"
+    hbm = peaks.get("hbm_gbs", 6650.0)
+    bf16 = peaks.get("bf16_tflops", 1590.0)
+    stream = ctx.stream
+    reps = max(args.steps, 10)
+    rows = []
+    with torch.cuda.stream(stream):
+        for e in log:
+            for _ in range(3):
+                relaunch(e)
+            stream.synchronize()
+            evs = []
+            for _ in range(reps):
+                flush.zero_()
+                a = torch.cuda.Event(enable_timing=True)
+                b = torch.cuda.Event(enable_timing=True)
+                a.record(stream)
+                relaunch(e)
+                b.record(stream)
+                evs.append((a, b))
+            stream.synchronize()
+            ms = statistics.mean(x.elapsed_time(y) for x, y in evs)
+            if e[0] == "transform":
+                t = e[1]
+                el = e[2].data.element_size()
+                nbytes = el * (t.elems_read + t.elems_written * (1 if e[5] == 0 else 2))
+                rows.append({"kernel": "treetransform", "ms": ms, "bytes": nbytes,
+                             "gbs": nbytes / (ms * 1e-3) / 1e9, "frac_hbm": nbytes / (ms * 1e-3) / 1e9 / hbm})
+            else:
+                plan = e[1]
+                S = plan.slices
+                rows.append({"kernel": "grouped_gemm_split" if S else "grouped_gemm_fp64", "ms": ms,
+                             "flops": plan.flops, "gflops": plan.flops / (ms * 1e-3) / 1e9, "slices": S})
+    dom = max(rows, key=lambda r: r["ms"])
+    total = sum(r["ms"] for r in rows)
+    for r in rows:
+        r["share"] = r["ms"] / total
+    if dom["kernel"] == "treetransform":
+        roof = {"kernel": "treetransform", "bound": "hbm", "achieved": dom["gbs"], "peak": hbm,
+                "unit": "GB/s", "frac": dom["gbs"] / hbm, "traffic": None,
+                "peak_source": f"hbm_gbs of {src} peaks"}
+    else:
+        S = dom.get("slices") or 0
+        if S:
+            ops = dom["flops"] * S * (S + 1) / 2
+            ach = ops / (dom["ms"] * 1e-3) / 1e12
+            peak = 2.0 * bf16
+            roof = {"kernel": "grouped_gemm_split (slice pass + int8 tensor-core products)",
+                    "bound": "tensor", "achieved": ach, "peak": peak, "unit": "TFLOP/s",
+                    "frac": ach / peak, "traffic": None,
+                    "peak_source": f"2 x bf16_tflops of {src} peaks (int8 dense = 2 x bf16 dense)",
+                    "algorithmic": f"S(S+1)/2 = {S * (S + 1) // 2} int8 products of 2mnk = {dom['flops']:.4e}",
+                    "fp64_equiv_gflops": dom["gflops"], "ms_per_launch": dom["ms"]}
+        else:
+            roof = {"kernel": "grouped_gemm_fp64", "bound": "tensor", "achieved": dom["gflops"] / 1e3,
+                    "peak": None, "unit": "TFLOP/s", "frac": None, "traffic": None}
+    return roof, rows
+
+
+def cpu_baseline(args, tens_o, flops):
+    """Oracle contraction on the host (numpy/BLAS, every host thread), bounded sample."""
+    t0 = time.perf_counter()
+    n = 0
+    while True:
+        oracle_eval(args.workload, tens_o)
+        n += 1
+        if time.perf_counter() - t0 > 10.0 or n >= 20:
+            break
+    dt = time.perf_counter() - t0
+    cores = os.cpu_count()
+    return {"value": flops * n / dt / 1e9, "unit": "GFLOP/s", "cores": cores, "kind": "port",
+            "sample": f"{n} full contractions of the same workload (oracle restatement, numpy/BLAS)"}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="su2_large", choices=sorted(WORKLOADS))
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -20,5 +20,6 @@ from .indexmanipulations import (permute, permute_, braid, braid_, transpose, tr
 from .linalg import mul_, compose, norm, tr, inner, dot, scale_, add_
 from .tensoroperations import (tensoradd_, tensorcontract_, tensorcontract, contract_,
                                tensor, tensorcontract_structure, tensoradd_structure)
+from .network import NetworkPlan
 
 __version__ = "0.1.0"

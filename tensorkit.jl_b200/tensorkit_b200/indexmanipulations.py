@@ -28,6 +28,26 @@ __all__ = ["permute", "permute_", "braid", "braid_", "add_transform_", "transpos
            "transpose_", "repartition", "device_table", "dtype_code"]
 
 
+# every device launch issued while this list is installed is recorded (used to re-time
+# individual kernels of a network)
+LAUNCH_LOG: list | None = None
+
+
+def relaunch(entry):
+    """Re-issue one recorded launch with the same operands (for kernel timing)."""
+    ctx = entry[1].ctx
+    if entry[0] == "transform":
+        _, table, tdst, tsrc, a, b, conj = entry
+        L.check(ctx.lib.tkb_treetransform(ctx.handle, table.handle, dtype_code(tdst.data),
+                                          C.c_void_p(tdst.data.data_ptr()), C.c_void_p(tsrc.data.data_ptr()),
+                                          _scalar(a), _scalar(b), conj), ctx.handle)
+    else:
+        _, plan, tC, tA, tB, a, b = entry
+        L.check(ctx.lib.tkb_grouped_gemm(ctx.handle, plan.handle, C.c_void_p(tC.data.data_ptr()),
+                                         C.c_void_p(tA.data.data_ptr()), C.c_void_p(tB.data.data_ptr()),
+                                         _scalar(a), _scalar(b)), ctx.handle)
+
+
 def dtype_code(t):
     import torch
     if t.dtype == torch.float64:
@@ -73,6 +93,8 @@ def add_transform_(tdst: TensorMap, tsrc, p, table: DeviceTable, alpha=1.0, beta
         raise TypeError("source and destination must share their scalar type")
     code = dtype_code(tdst.data)
     conj = 1 if (isinstance(tsrc, AdjointTensorMap) and tsrc.is_complex()) else 0
+    if LAUNCH_LOG is not None:
+        LAUNCH_LOG.append(("transform", table, tdst, tsrc, complex(alpha), complex(beta), conj))
     _sync_in(ctx, tdst, tsrc)
     L.check(ctx.lib.tkb_treetransform(ctx.handle, table.handle, code,
                                       C.c_void_p(tdst.data.data_ptr()),

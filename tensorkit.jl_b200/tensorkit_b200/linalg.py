@@ -24,6 +24,10 @@ __all__ = ["mul_", "compose", "norm", "tr", "inner", "dot", "scale_", "add_", "g
            "block_gemm_descriptors"]
 
 
+# algorithmic flops of every grouped GEMM issued while this list is installed
+FLOP_LOG: list | None = None
+
+
 def _operand_blocks(t):
     """{c: (offset, rows, cols, ld, op)} for op(block) of a TensorMap or lazy adjoint."""
     out = {}
@@ -87,6 +91,11 @@ def mul_(tC: TensorMap, tA, tB, alpha=1.0, beta=0.0, prec=None, slices=None):
         raise TypeError("mul! operands must share their scalar type")
     ctx = get_context(tC.data.device.index)
     plan = gemm_plan(ctx, tC, tA, tB, prec, slices)
+    if FLOP_LOG is not None:
+        FLOP_LOG.append(plan.flops)
+    from . import indexmanipulations as _im
+    if _im.LAUNCH_LOG is not None:
+        _im.LAUNCH_LOG.append(("gemm", plan, tC, tA, tB, complex(alpha), complex(beta)))
     _sync_in(ctx)
     L.check(ctx.lib.tkb_grouped_gemm(ctx.handle, plan.handle, C.c_void_p(tC.data.data_ptr()),
                                      C.c_void_p(tA.data.data_ptr()), C.c_void_p(tB.data.data_ptr()),
