@@ -138,6 +138,24 @@ int tkb_reduce(tkb_ctx *ctx, const tkb_rplan *plan, int kind, int dtype, const v
 int tkb_reduce_async(tkb_ctx *ctx, const tkb_rplan *plan, int kind, int dtype,
                      const void *x, const void *y, double *dev_out);
 
+/* Allocation-free variant of tkb_reduce. It has no counterpart in the reference: it exists
+ * for callers that cannot call cudaMalloc at all — code whose device memory is owned
+ * entirely by another allocator (a Julia CUDA.jl memory pool, a framework that has reserved
+ * the whole device) or code running where a device allocation may block or fail (a
+ * finalizer, an out-of-memory recovery path). It needs no context, plan or workspace and
+ * calls no allocating routine: its scratch (segment table, per-block partial sums, result;
+ * about 57 KiB) is a static device array that every GPU loading the library holds until the
+ * process exits. The caller passes the data vectors and host segment arrays (same meaning
+ * as tkb_rplan_create) and receives (re, im) in host_out after the stream has completed.
+ * Limits: at most 1024 segments (TKB_ERR_SIZE beyond that). The first call on a device
+ * looks up the array's device address for that device; make that first call before any
+ * stream capture. All calls share the array, so calls that overlap on the GPU (other
+ * streams, other host threads) race and must be serialised by the caller. */
+int tkb_reduce_noalloc(int device, void *stream, int kind, int dtype, const void *x,
+                       const void *y, int64_t len, int64_t nseg, const int64_t *off,
+                       const int64_t *count, const int64_t *stride, const double *weight,
+                       double *host_out);
+
 /* ---- CUDA graph capture of a sequence of calls on the context stream ---------------- */
 int tkb_graph_begin(tkb_ctx *ctx);
 int tkb_graph_end(tkb_ctx *ctx, tkb_graph **out);

@@ -3,6 +3,8 @@
 // Two deterministic passes: per-CTA partial sums over contiguous ranges of the segment
 // element space, then one CTA sums the partials in a fixed order.
 #include <algorithm>
+#include <mutex>
+#include <string>
 
 #include "tkb_internal.h"
 
@@ -81,6 +83,109 @@ __global__ void __launch_bounds__(RT) reduce_final_kernel(const double2 *__restr
 }
 
 }  // namespace
+
+// ---- allocation-free variant ------------------------------------------------------------
+// Scratch for tkb_reduce_noalloc: segment table, prefix sums, per-CTA partials and the
+// result, in one file-scope device array that every GPU loading the library holds until
+// the process exits. Host code only sees a stand-in for this symbol; its device address
+// comes from cudaGetSymbolAddress, taken once per device.
+namespace {
+constexpr int64_t kNoAllocMaxSeg = 1024;
+constexpr int kNoAllocMaxCta = 1024;
+constexpr size_t kNoAllocSegBytes = kNoAllocMaxSeg * sizeof(RSeg);                 // 32 KiB
+constexpr size_t kNoAllocBeginOff = kNoAllocSegBytes;
+constexpr size_t kNoAllocPartialOff = (kNoAllocBeginOff + (kNoAllocMaxSeg + 1) * 8 + 255) / 256 * 256;
+constexpr size_t kNoAllocResultOff = kNoAllocPartialOff + kNoAllocMaxCta * sizeof(double2);
+constexpr size_t kNoAllocBytes = kNoAllocResultOff + 256;                          // ~57 KiB
+}  // namespace
+
+static __device__ __align__(256) unsigned char tkb_noalloc_scratch[kNoAllocBytes];
+
+namespace {
+std::mutex g_noalloc_mu;
+void *g_noalloc_ptr[64] = {nullptr};
+}  // namespace
+
+extern "C" int tkb_reduce_noalloc(int device, void *stream, int kind, int dtype, const void *x,
+                                  const void *y, int64_t len, int64_t nseg, const int64_t *off,
+                                  const int64_t *count, const int64_t *stride, const double *weight,
+                                  double *host_out) {
+  if (kind < TKB_NORM2 || kind > TKB_TRACE) return tkb_set_error(nullptr, TKB_ERR_ARG, "unknown reduction");
+  if (dtype != TKB_F64 && dtype != TKB_C128) return tkb_set_error(nullptr, TKB_ERR_ARG, "unknown dtype");
+  if (!host_out) return tkb_set_error(nullptr, TKB_ERR_ARG, "null output");
+  if (device < 0 || device >= 64) return tkb_set_error(nullptr, TKB_ERR_ARG, "device out of range");
+  if (nseg < 0 || nseg > kNoAllocMaxSeg)
+    return tkb_set_error(nullptr, TKB_ERR_SIZE,
+                         "tkb_reduce_noalloc supports at most 1024 segments (got " +
+                             std::to_string(nseg) + "); use tkb_reduce for larger tensors");
+  if (nseg > 0 && (!off || !count || !stride || !weight))
+    return tkb_set_error(nullptr, TKB_ERR_ARG, "null segment array");
+  // host-side staging on the stack (no heap, no device allocation)
+  RSeg segs[kNoAllocMaxSeg];
+  int64_t begin[kNoAllocMaxSeg + 1];
+  begin[0] = 0;
+  for (int64_t s = 0; s < nseg; ++s) {
+    if (count[s] < 0 || off[s] < 0 || stride[s] < 0)
+      return tkb_set_error(nullptr, TKB_ERR_ARG, "invalid segment");
+    if (count[s] > 0 && off[s] + (count[s] - 1) * stride[s] >= len)
+      return tkb_set_error(nullptr, TKB_ERR_SIZE, "segment outside the data vector");
+    segs[s] = {off[s], count[s], stride[s], weight[s]};
+    begin[s + 1] = begin[s] + count[s];
+  }
+  const int64_t total = begin[nseg];
+  if (total > 0 && (!x || (kind == TKB_INNER && !y)))
+    return tkb_set_error(nullptr, TKB_ERR_ARG, "null data");
+
+  int prev = 0;
+  if (cudaGetDevice(&prev) != cudaSuccess) prev = device;
+  cudaError_t e = cudaSetDevice(device);
+  if (e != cudaSuccess) return tkb_set_error(nullptr, TKB_ERR_CUDA, cudaGetErrorString(e));
+  unsigned char *base = nullptr;
+  {
+    std::lock_guard<std::mutex> lk(g_noalloc_mu);
+    if (!g_noalloc_ptr[device]) {
+      void *p = nullptr;
+      e = cudaGetSymbolAddress(&p, tkb_noalloc_scratch);
+      if (e != cudaSuccess) {
+        cudaSetDevice(prev);
+        return tkb_set_error(nullptr, TKB_ERR_CUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
+      }
+      g_noalloc_ptr[device] = p;
+    }
+    base = static_cast<unsigned char *>(g_noalloc_ptr[device]);
+  }
+  cudaStream_t st = (cudaStream_t)stream;
+  RSeg *dsegs = reinterpret_cast<RSeg *>(base);
+  int64_t *dbegin = reinterpret_cast<int64_t *>(base + kNoAllocBeginOff);
+  double2 *dpart = reinterpret_cast<double2 *>(base + kNoAllocPartialOff);
+  double *dres = reinterpret_cast<double *>(base + kNoAllocResultOff);
+  e = cudaSuccess;
+  if (total == 0) {
+    host_out[0] = 0.0;
+    host_out[1] = 0.0;
+  } else {
+    // pageable host sources: the copies have read the stack buffers when these calls return
+    e = cudaMemcpyAsync(dsegs, segs, nseg * sizeof(RSeg), cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(dbegin, begin, (nseg + 1) * sizeof(int64_t), cudaMemcpyHostToDevice, st);
+    const int nb = (int)std::max<int64_t>(1, std::min<int64_t>((total + 4095) / 4096, kNoAllocMaxCta));
+    if (e == cudaSuccess) {
+      if (dtype == TKB_F64)
+        reduce_partial_kernel<double><<<nb, RT, 0, st>>>(dsegs, dbegin, nseg, total, kind,
+                                                         (const double *)x, (const double *)y, dpart);
+      else
+        reduce_partial_kernel<double2><<<nb, RT, 0, st>>>(dsegs, dbegin, nseg, total, kind,
+                                                          (const double2 *)x, (const double2 *)y, dpart);
+      reduce_final_kernel<<<1, RT, 0, st>>>(dpart, nb, dres);
+      e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaMemcpyAsync(host_out, dres, 2 * sizeof(double), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  }
+  cudaSetDevice(prev);
+  if (e != cudaSuccess) return tkb_set_error(nullptr, TKB_ERR_CUDA, cudaGetErrorString(e));
+  return TKB_OK;
+}
 
 int tkb_reduce_launch(tkb_ctx *ctx, const tkb_rplan *p, int kind, int dtype, const void *x,
                       const void *y, double *dev_out) {

@@ -27,7 +27,8 @@ EXPORTS = [
     "tkb_ctx_synchronize", "tkb_ctx_launch_count", "tkb_last_error", "tkb_table_create",
     "tkb_table_destroy", "tkb_table_info", "tkb_treetransform", "tkb_gemm_plan_create",
     "tkb_gemm_plan_destroy", "tkb_gemm_plan_info", "tkb_grouped_gemm", "tkb_rplan_create",
-    "tkb_rplan_destroy", "tkb_reduce", "tkb_reduce_async", "tkb_graph_begin", "tkb_graph_end",
+    "tkb_rplan_destroy", "tkb_reduce", "tkb_reduce_async", "tkb_reduce_noalloc",
+    "tkb_graph_begin", "tkb_graph_end",
     "tkb_graph_launch", "tkb_graph_destroy",
 ]
 
@@ -90,6 +91,8 @@ def _declare(lib):
         "tkb_rplan_destroy": ([vp], C.c_int),
         "tkb_reduce": ([vp, vp, C.c_int, C.c_int, vp, vp, P(dbl)], C.c_int),
         "tkb_reduce_async": ([vp, vp, C.c_int, C.c_int, vp, vp, vp], C.c_int),
+        "tkb_reduce_noalloc": ([C.c_int, vp, C.c_int, C.c_int, vp, vp, i64, i64, vp, vp, vp, vp,
+                                P(dbl)], C.c_int),
         "tkb_graph_begin": ([vp], C.c_int),
         "tkb_graph_end": ([vp, P(vp)], C.c_int),
         "tkb_graph_launch": ([vp, vp], C.c_int),
