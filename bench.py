@@ -419,12 +419,52 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="su2_large", choices=sorted(WORKLOADS))
+    ap.add_argument("--kernel-only", default=None, choices=["transform", "gemm"],
+                    help="profiling aid: one eager step, then relaunch the largest kernel of this kind")
+    ap.add_argument("--precision", default="split", choices=["split", "plain"])
+    ap.add_argument("--reps", type=int, default=3)
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
     if args.impl == "reference":
         return run_reference(args)
+    if args.kernel_only:
+        return run_kernel_only(args)
     return run_ours(args)
+
+
+def run_kernel_only(args):
+    """One eager step (every table and plan built, all launches recorded), then the largest
+    launch of the requested kind relaunched `--reps` times. Prints how many launches of that
+    kernel preceded the relaunches, for `ncu -k ... -s <skip>`."""
+    import torch
+    import tensorkit_b200 as tk
+    from helpers import to_device
+    from tensorkit_b200 import indexmanipulations as IM
+
+    dev = torch.device("cuda", 0)
+    inputs = {k: to_device(v, dev) for k, v in oracle_inputs(args.workload).items()}
+    ctx = tk.get_context(0)
+    p = tk.NetworkPlan(WORKLOADS[args.workload]["expr"], precision=args.precision, **inputs)
+    IM.LAUNCH_LOG = []
+    p.run_eager()
+    log, IM.LAUNCH_LOG = IM.LAUNCH_LOG, None
+    kind = args.kernel_only
+    cands = [e for e in log if e[0] == kind]
+    if kind == "transform":
+        big = max(cands, key=lambda e: e[1].elems_read + e[1].elems_written)
+        size = {"elems_read": big[1].elems_read, "elems_written": big[1].elems_written,
+                "ntasks": big[1].ntasks}
+    else:
+        big = max(cands, key=lambda e: e[1].flops)
+        size = {"flops": big[1].flops, "slices": big[1].slices}
+    with torch.cuda.stream(ctx.stream):
+        for _ in range(args.reps):
+            IM.relaunch(big)
+    ctx.stream.synchronize()
+    print(json.dumps({"kernel_only": kind, "workload": args.workload, "preceding_launches": len(cands),
+                      "reps": args.reps, **size}))
+    return 0
 
 
 if __name__ == "__main__":

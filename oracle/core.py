@@ -251,9 +251,15 @@ class Space:
 
 
 class Hom:
-    def __init__(self, cod, dom):
+    """cod ← dom; `u` (the unit sector) is carried explicitly so that spaces without legs
+    (scalars) keep their sector type."""
+
+    def __init__(self, cod, dom, u=None):
         self.cod = tuple(cod)
         self.dom = tuple(dom)
+        if u is None:
+            u = unit((self.cod + self.dom)[0].keys[0])
+        self.u = u
 
     def n1(self):
         return len(self.cod)
@@ -265,19 +271,19 @@ class Hom:
         return self.cod[i - 1] if i <= len(self.cod) else self.dom[i - 1 - len(self.cod)].flipdual()
 
     def select(self, p):
-        return Hom([self.leg(i) for i in p[0]], [self.leg(i).flipdual() for i in p[1]])
+        return Hom([self.leg(i) for i in p[0]], [self.leg(i).flipdual() for i in p[1]], self.u)
 
     def adjoint(self):
-        return Hom(self.dom, self.cod)
+        return Hom(self.dom, self.cod, self.u)
 
     def __eq__(self, o):
-        return self.cod == o.cod and self.dom == o.dom
+        return self.cod == o.cod and self.dom == o.dom and self.u == o.u
 
     def __hash__(self):
-        return hash((self.cod, self.dom))
+        return hash((self.cod, self.dom, self.u))
 
     def unit(self):
-        return unit((self.cod + self.dom)[0].keys[0])
+        return self.u
 
 
 def _product(lists):
@@ -594,7 +600,7 @@ def mul(A: BT, B: BT, adjA=False, adjB=False):
     WA = A.W.adjoint() if adjA else A.W
     WB = B.W.adjoint() if adjB else B.W
     assert WA.dom == WB.cod
-    WC = Hom(WA.cod, WB.dom)
+    WC = Hom(WA.cod, WB.dom, WA.unit())
     dt = np.result_type(A.data, B.data)
     C = BT(WC, np.zeros(layout(WC)[0], dtype=dt))
     bA = A.blocks()

@@ -145,7 +145,7 @@ int tkb_gemm_plan_create(tkb_ctx *ctx, const tkb_gemm_desc *d, tkb_plan **out) {
   p->lenA = d->lenA;
   p->lenB = d->lenB;
   p->lenC = d->lenC;
-  std::vector<GTile> tiles;
+  std::vector<GTile> tiles, sk;
   double flops = 0;
   for (int64_t i = 0; i < nb; ++i) {
     GBlock b;
@@ -173,12 +173,20 @@ int tkb_gemm_plan_create(tkb_ctx *ctx, const tkb_gemm_desc *d, tkb_plan **out) {
       if (b.opB == TKB_OP_C) b.opB = TKB_OP_T;
     }
     flops += (d->dtype == TKB_C128 ? 8.0 : 2.0) * (double)b.m * (double)b.n * (double)b.k;
+    b.skinny = (b.n <= kSkinnyMax && b.k <= kSkinnyMax) ? 1 : 0;
     p->hblocks.push_back(b);
-    if (b.m > 0 && b.n > 0)
-      for (int64_t m0 = 0; m0 < b.m; m0 += 64)
-        for (int64_t n0 = 0; n0 < b.n; n0 += 64)
-          tiles.push_back({(int32_t)i, (int32_t)m0, (int32_t)n0, b.k > 0 ? 0 : 1});
+    if (b.m > 0 && b.n > 0) {
+      if (b.skinny) {
+        for (int64_t m0 = 0; m0 < b.m; m0 += kSkinnyRows)
+          sk.push_back({(int32_t)i, (int32_t)m0, 0, b.k > 0 ? 0 : 1});
+      } else {
+        for (int64_t m0 = 0; m0 < b.m; m0 += 64)
+          for (int64_t n0 = 0; n0 < b.n; n0 += 64)
+            tiles.push_back({(int32_t)i, (int32_t)m0, (int32_t)n0, b.k > 0 ? 0 : 1});
+      }
+    }
   }
+  p->nsk = (int64_t)sk.size();
   std::stable_sort(tiles.begin(), tiles.end(), [&](const GTile &x, const GTile &y) {
     return p->hblocks[x.block].k > p->hblocks[y.block].k;
   });
@@ -200,6 +208,10 @@ int tkb_gemm_plan_create(tkb_ctx *ctx, const tkb_gemm_desc *d, tkb_plan **out) {
     e = cudaMalloc((void **)&p->tiles, tiles.size() * sizeof(GTile));
     if (e == cudaSuccess) e = cudaMemcpy(p->tiles, tiles.data(), tiles.size() * sizeof(GTile), cudaMemcpyHostToDevice);
   }
+  if (e == cudaSuccess && !sk.empty()) {
+    e = cudaMalloc((void **)&p->sktasks, sk.size() * sizeof(GTile));
+    if (e == cudaSuccess) e = cudaMemcpy(p->sktasks, sk.data(), sk.size() * sizeof(GTile), cudaMemcpyHostToDevice);
+  }
   if (e != cudaSuccess) {
     tkb_gemm_plan_destroy(p);
     return tkb_set_error(ctx, TKB_ERR_CUDA, std::string("plan upload: ") + cudaGetErrorString(e));
@@ -212,6 +224,7 @@ int tkb_gemm_plan_destroy(tkb_plan *p) {
   if (!p) return TKB_OK;
   cudaFree(p->blocks);
   cudaFree(p->tiles);
+  cudaFree(p->sktasks);
   cudaFree(p->stiles);
   cudaFree(p->sjobs);
   cudaFree(p->srow_begin);
@@ -232,6 +245,8 @@ int tkb_grouped_gemm(tkb_ctx *ctx, const tkb_plan *p, void *C, const void *A, co
   if (p->owner != ctx) return tkb_set_error(ctx, TKB_ERR_ARG, "plan belongs to another context");
   if (p->nblocks > 0 && (!C || (p->flops > 0 && (!A || !B))))
     return tkb_set_error(ctx, TKB_ERR_ARG, "null data pointer");
+  const int rc = tkb_gemm_skinny_launch(ctx, p, C, A, B, alpha, beta);
+  if (rc != TKB_OK) return rc;
   if (p->precision == TKB_SPLIT_INT8) return tkb_gemm_split_launch(ctx, p, C, A, B, alpha, beta);
   return tkb_gemm_launch(ctx, p, C, A, B, alpha, beta);
 }

@@ -341,7 +341,97 @@ __global__ void __launch_bounds__(256)
   }
 }
 
+// ---- skinny blocks (n, k ≤ 16): one thread per output row, op(B) in shared memory -----------
+// Such blocks (tall-skinny GEMMs against small MPO bonds) are bound by reading op(A) and
+// writing C; the row kernel streams both exactly once with coalesced accesses for op N.
+template <typename T>
+__device__ __forceinline__ T ldA(const T *p, bool conj);
+template <>
+__device__ __forceinline__ double ldA<double>(const double *p, bool) { return __ldg(p); }
+template <>
+__device__ __forceinline__ double2 ldA<double2>(const double2 *p, bool conj) {
+  double2 v = __ldg(p);
+  if (conj) v.y = -v.y;
+  return v;
+}
+__device__ __forceinline__ double mac(double a, double b, double c) { return fma(a, b, c); }
+__device__ __forceinline__ double2 mac(double2 a, double2 b, double2 c) {
+  return make_double2(fma(a.x, b.x, fma(-a.y, b.y, c.x)), fma(a.x, b.y, fma(a.y, b.x, c.y)));
+}
+template <typename T>
+__device__ __forceinline__ T make_beta(CDbl b);
+template <>
+__device__ __forceinline__ double make_beta<double>(CDbl b) { return b.x; }
+template <>
+__device__ __forceinline__ double2 make_beta<double2>(CDbl b) { return make_double2(b.x, b.y); }
+__device__ __forceinline__ double zero(double) { return 0.0; }
+__device__ __forceinline__ double2 zero(double2) { return make_double2(0.0, 0.0); }
+__device__ __forceinline__ double scl(double v, CDbl a) { return a.x * v; }
+__device__ __forceinline__ double2 scl(double2 v, CDbl a) {
+  return make_double2(a.x * v.x - a.y * v.y, a.x * v.y + a.y * v.x);
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kSkinnyRows)
+    gemm_skinny_kernel(const GBlock *__restrict__ blocks, const GTile *__restrict__ tasks, int64_t ntasks,
+                       T *__restrict__ C, const T *__restrict__ A, const T *__restrict__ B, CDbl alpha,
+                       CDbl beta) {
+  __shared__ T Bs[kSkinnyMax * kSkinnyMax];
+  const bool bz = beta.x == 0.0 && beta.y == 0.0;
+  for (int64_t ti = blockIdx.x; ti < ntasks; ti += gridDim.x) {
+    const GTile tk = tasks[ti];
+    const GBlock b = blocks[tk.block];
+    const int n = (int)b.n, k = (int)b.k;
+    __syncthreads();
+    for (int e = threadIdx.x; e < k * n; e += blockDim.x) {
+      const int l = e % k, j = e / k;  // op(B)(l, j)
+      const int64_t idx = (b.opB == TKB_OP_N) ? b.offB + l + (int64_t)j * b.ldb : b.offB + j + (int64_t)l * b.ldb;
+      Bs[l + j * kSkinnyMax] = ldA<T>(B + idx, b.opB == TKB_OP_C);
+    }
+    __syncthreads();
+    const int64_t i = tk.m0 + threadIdx.x;
+    if (i >= b.m) continue;
+    T acc[kSkinnyMax];
+#pragma unroll
+    for (int j = 0; j < kSkinnyMax; ++j) acc[j] = zero(T{});
+    if (tk.kind == 0) {
+      for (int l = 0; l < k; ++l) {
+        const int64_t ia = (b.opA == TKB_OP_N) ? b.offA + i + (int64_t)l * b.lda : b.offA + l + i * b.lda;
+        const T a = ldA<T>(A + ia, b.opA == TKB_OP_C);
+#pragma unroll
+        for (int j = 0; j < kSkinnyMax; ++j)
+          if (j < n) acc[j] = mac(a, Bs[l + j * kSkinnyMax], acc[j]);
+      }
+    }
+#pragma unroll
+    for (int j = 0; j < kSkinnyMax; ++j) {
+      if (j < n) {
+        T *p = C + b.offC + i + (int64_t)j * b.ldc;
+        T r = scl(acc[j], alpha);
+        if (!bz) r = mac(*p, make_beta<T>(beta), r);
+        *p = r;
+      }
+    }
+  }
+}
+
 }  // namespace
+
+int tkb_gemm_skinny_launch(tkb_ctx *ctx, const tkb_plan *p, void *C, const void *A,
+                           const void *B, tkb_scalar alpha, tkb_scalar beta) {
+  if (p->nsk == 0) return TKB_OK;
+  const int grid = (int)std::min<int64_t>(p->nsk, (int64_t)ctx->num_sms * 8);
+  const CDbl a{alpha.re, alpha.im}, bb{beta.re, beta.im};
+  if (p->dtype == TKB_F64)
+    gemm_skinny_kernel<double><<<grid, kSkinnyRows, 0, ctx->stream>>>(
+        p->blocks, p->sktasks, p->nsk, (double *)C, (const double *)A, (const double *)B, a, bb);
+  else
+    gemm_skinny_kernel<double2><<<grid, kSkinnyRows, 0, ctx->stream>>>(
+        p->blocks, p->sktasks, p->nsk, (double2 *)C, (const double2 *)A, (const double2 *)B, a, bb);
+  ctx->launches++;
+  TKB_CUDA_TRY(ctx, cudaGetLastError());
+  return TKB_OK;
+}
 
 int tkb_gemm_launch(tkb_ctx *ctx, const tkb_plan *p, void *C, const void *A, const void *B,
                     tkb_scalar alpha, tkb_scalar beta) {

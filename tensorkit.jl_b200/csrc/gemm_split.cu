@@ -15,10 +15,23 @@
 // row pairs (2r, 2r+1) = ([Re A_r, -Im A_r], [Im A_r, Re A_r]) and op(B) the 2k×n matrix
 // [Re B; Im B], so rows 2r and 2r+1 of the real result are Re and Im of C_r.
 //
-// Launches: slice pass (all operand rows of all blocks, one warp per row) + product pass
-// (persistent CTAs over a cost-ordered tile queue, 64×64 output tiles).
+// Slice layout in the workspace: per block, per slice, the rows of op(A) (op(B)ᵀ) are cut
+// into panels of 128 (64) rows; a panel is a sequence of 64-byte K stages, each stored as
+// the canonical K-major "core matrix" layout of the tensor-core operand descriptors
+// (8-row × 16-byte core matrices; 512 bytes between 8-row groups, 128 bytes between the
+// four 16-byte K chunks). One stage of one slice is therefore one contiguous 8 KiB (4 KiB)
+// block that a single bulk copy moves into shared memory.
+//
+// Launches: slice pass (one warp per 32 operand rows) + product pass:
+//   tcgen05 kernel (default): one CTA per 128×64 output tile; one thread streams the
+//   S slice stages of A and B with cp.async.bulk into a two-stage shared-memory ring and
+//   issues tcgen05.mma.kind::i8 (M=128, N=64, K=32) into S int32 accumulators held in
+//   tensor memory (S·64 of 512 columns); four warps read the accumulators back with
+//   tcgen05.ld and recombine them in FP64.
+//   mma.sync kernel (TKB_SPLIT_KERNEL=mma): the same products with int8 mma.sync.
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <numeric>
 
@@ -26,8 +39,8 @@
 
 namespace {
 
-constexpr int SBM = 64, SBN = 64, SBK = 32;  // SBK: bytes (int8 elements) of K per step
-constexpr int SPITCH = 48;                    // smem row pitch in bytes: conflict-free frags
+constexpr int PANEL_A = 128, PANEL_B = 64;   // rows per panel
+constexpr int KSTAGE = 64;                   // bytes of K per stage
 constexpr int SMAX = 7;
 
 struct SliceJob {
@@ -38,6 +51,14 @@ struct SliceJob {
 struct CDbl {
   double x, y;
 };
+
+// byte offset of (row r, K byte kb) inside one slice plane
+__host__ __device__ __forceinline__ int64_t slice_off(int64_t r, int64_t kb, int64_t kpad, int pr) {
+  const int64_t panel = r / pr, rr = r % pr;
+  const int64_t stg = kb >> 6, kk = kb & 63;
+  return panel * (pr * kpad) + stg * (pr * KSTAGE) + (rr >> 3) * 512 + (kk >> 4) * 128 +
+         (rr & 7) * 16 + (kk & 15);
+}
 
 // element (r, l) of the logical real operand (rows r of M' or N', column l of K')
 __device__ __forceinline__ double op_elem(const GBlock &b, int operand, int cplx,
@@ -70,59 +91,371 @@ __device__ __forceinline__ double op_elem(const GBlock &b, int operand, int cplx
   return (b.opB == TKB_OP_C) ? -im : im;
 }
 
-// One warp per logical row of every operand of every block (rows enumerated through the
-// row_begin prefix sums, padding rows included so the padded slices are zero-filled).
+// One CTA (8 warps) per group of 32 operand rows (rows of all jobs enumerated through the
+// group prefix sums; padding rows included so padded slices are zero-filled).
+// Row-contiguous operands (real op(A) = A, real op(B) = Bᵀ) use lane = row: the K range is
+// cut into 16-element chunks dealt round-robin to the 8 warps, loads are coalesced across
+// lanes (16 independent loads per lane per chunk), the row maxima are combined through
+// shared memory, and each lane packs 16 K bytes per slice into one 16-byte store.
+// Other operands use lane = K position, four rows per warp.
+template <int S>
 __global__ void __launch_bounds__(256)
-    slice_kernel(const GBlock *__restrict__ blocks, const int64_t *__restrict__ row_begin,
-                 const SliceJob *__restrict__ jobs, int njobs, int64_t nrows, int S, int cplx,
+    slice_kernel(const GBlock *__restrict__ blocks, const int64_t *__restrict__ grp_begin,
+                 const SliceJob *__restrict__ jobs, int njobs, int64_t ngroups, int cplx,
                  const double *__restrict__ A, const double *__restrict__ B, int8_t *ws) {
-  const int lane = threadIdx.x & 31;
-  const int64_t wid = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
-  const int64_t nw = (int64_t)gridDim.x * (blockDim.x >> 5);
-  for (int64_t row = wid; row < nrows; row += nw) {
+  __shared__ double red[8][32];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (int64_t grp = blockIdx.x; grp < ngroups; grp += gridDim.x) {
     int lo = 0, hi = njobs - 1;
     while (lo < hi) {
       const int mid = (lo + hi + 1) >> 1;
-      if (row_begin[mid] <= row) lo = mid; else hi = mid - 1;
+      if (grp_begin[mid] <= grp) lo = mid; else hi = mid - 1;
     }
     const SliceJob job = jobs[lo];
     const GBlock &b = blocks[job.block];
-    const int64_t r = row - row_begin[lo];
-    const int64_t Mlog = job.operand == 0 ? (cplx ? 2 * b.m : b.m) : b.n;
+    const int64_t r0 = (grp - grp_begin[lo]) * 32;
+    const int op = job.operand;
+    const int64_t Mlog = op == 0 ? (cplx ? 2 * b.m : b.m) : b.n;
     const int64_t Klog = cplx ? 2 * b.k : b.k;
-    const int64_t rows_pad = job.operand == 0 ? b.mpad : b.npad;
+    const int64_t rows_pad = op == 0 ? b.mpad : b.npad;
+    const int pr = op == 0 ? PANEL_A : PANEL_B;
     const int64_t kpad = b.kpad;
-    int8_t *base = ws + (job.operand == 0 ? b.wsA : b.wsB);
-    int32_t *expo = reinterpret_cast<int32_t *>(ws + (job.operand == 0 ? b.wsEA : b.wsEB));
-    const double *X = job.operand == 0 ? A : B;
-    const bool valid = r < Mlog;
-    double mx = 0.0;
-    if (valid) {
-      for (int64_t l = lane; l < Klog; l += 32)
-        mx = fmax(mx, fabs(op_elem(b, job.operand, cplx, X, r, l)));
-      if (cplx && job.operand == 0) {  // a complex row pair shares one exponent
-        for (int64_t l = lane; l < Klog; l += 32)
-          mx = fmax(mx, fabs(op_elem(b, job.operand, cplx, X, r ^ 1, l)));
+    int8_t *base = ws + (op == 0 ? b.wsA : b.wsB);
+    int32_t *expo = reinterpret_cast<int32_t *>(ws + (op == 0 ? b.wsEA : b.wsEB));
+    const double *X = op == 0 ? A : B;
+    const int64_t plane = rows_pad * kpad;
+    const bool row_contig = !cplx && ((op == 0 && b.opA == TKB_OP_N) || (op == 1 && b.opB != TKB_OP_N));
+    if (row_contig) {
+      // element (r, l) at X[xo + r + l * ld]
+      const int64_t xo = op == 0 ? b.offA : b.offB;
+      const int64_t ld = op == 0 ? b.lda : b.ldb;
+      const int64_t r = r0 + lane;
+      const bool valid = r < Mlog;
+      const int64_t nchunk = (Klog + 15) / 16;
+      double mx = 0.0;
+      if (valid) {
+        for (int64_t c = warp; c < nchunk; c += 8) {
+          double v[16];
+#pragma unroll
+          for (int q = 0; q < 16; ++q) {
+            const int64_t l = c * 16 + q;
+            v[q] = l < Klog ? X[xo + r + l * ld] : 0.0;
+          }
+#pragma unroll
+          for (int q = 0; q < 16; ++q) mx = fmax(mx, fabs(v[q]));
+        }
+      }
+      red[warp][lane] = mx;
+      __syncthreads();
+      mx = 0.0;
+#pragma unroll
+      for (int w = 0; w < 8; ++w) mx = fmax(mx, red[w][lane]);
+      __syncthreads();
+      int e = 0;
+      if (mx > 0.0) frexp(mx, &e);  // mx < 2^e
+      if (warp == 0) expo[r] = e;
+      for (int64_t c = warp; c < kpad / 16; c += 8) {
+        const int64_t l0 = c * 16;
+        double v[16];
+#pragma unroll
+        for (int q = 0; q < 16; ++q) {
+          const int64_t l = l0 + q;
+          v[q] = (valid && l < Klog) ? X[xo + r + l * ld] : 0.0;
+        }
+        uint32_t w[S][4];
+#pragma unroll
+        for (int s = 0; s < S; ++s) w[s][0] = w[s][1] = w[s][2] = w[s][3] = 0u;
+#pragma unroll
+        for (int q = 0; q < 16; ++q) {
+          double x = ldexp(v[q], -e);
+#pragma unroll
+          for (int s = 0; s < S; ++s) {
+            x *= 128.0;
+            const double qd = trunc(x);
+            x -= qd;
+            w[s][q >> 2] |= ((uint32_t)(uint8_t)(int8_t)qd) << (8 * (q & 3));
+          }
+        }
+        const int64_t off = slice_off(r, l0, kpad, pr);
+#pragma unroll
+        for (int s = 0; s < S; ++s)
+          *reinterpret_cast<uint4 *>(base + s * plane + off) = make_uint4(w[s][0], w[s][1], w[s][2], w[s][3]);
+      }
+      continue;
+    }
+    for (int rr = warp * 4; rr < warp * 4 + 4; ++rr) {
+      const int64_t r = r0 + rr;
+      const bool valid = r < Mlog;
+      double mx = 0.0;
+      if (valid) {
+        for (int64_t l = lane; l < Klog; l += 32) mx = fmax(mx, fabs(op_elem(b, op, cplx, X, r, l)));
+        if (cplx && op == 0)  // a complex row pair shares one exponent
+          for (int64_t l = lane; l < Klog; l += 32) mx = fmax(mx, fabs(op_elem(b, op, cplx, X, r ^ 1, l)));
+      }
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+      int e = 0;
+      if (mx > 0.0) frexp(mx, &e);
+      if (lane == 0) expo[r] = e;
+      for (int64_t l = lane; l < kpad; l += 32) {
+        double x = (valid && l < Klog) ? ldexp(op_elem(b, op, cplx, X, r, l), -e) : 0.0;
+        const int64_t off = slice_off(r, l, kpad, pr);
+#pragma unroll
+        for (int s = 0; s < S; ++s) {
+          x *= 128.0;
+          const double qd = trunc(x);
+          x -= qd;
+          base[s * plane + off] = (int8_t)qd;
+        }
+      }
+    }
+  }
+}
+
+// ---- shared epilogue: recombine one output value --------------------------------------------
+__device__ __forceinline__ void store_out(double v, int64_t i, int64_t j, const GBlock &b, int cplx,
+                                          double *C, CDbl alpha, CDbl beta, bool bz, int lane_xor) {
+  const int64_t Mreal = cplx ? 2 * b.m : b.m;
+  if (!cplx) {
+    if (i < b.m && j < b.n) {
+      double *p = C + b.offC + i + j * b.ldc;
+      double r = alpha.x * v;
+      if (!bz) r = fma(beta.x, *p, r);
+      *p = r;
+    }
+    return;
+  }
+  const double w = __shfl_xor_sync(0xffffffffu, v, lane_xor);  // partner row i ^ 1
+  if (!(i & 1) && i < Mreal && j < b.n) {
+    double2 *p = reinterpret_cast<double2 *>(C) + b.offC + (i >> 1) + j * b.ldc;
+    double rr = alpha.x * v - alpha.y * w;
+    double ri = alpha.x * w + alpha.y * v;
+    if (!bz) {
+      const double2 o = *p;
+      rr = fma(beta.x, o.x, fma(-beta.y, o.y, rr));
+      ri = fma(beta.x, o.y, fma(beta.y, o.x, ri));
+    }
+    *p = make_double2(rr, ri);
+  }
+}
+
+// ---- tcgen05 product kernel --------------------------------------------------------------------
+__device__ __forceinline__ uint32_t smem_u32(const void *p) {
+  return (uint32_t)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(count));
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ uint64_t globaltimer_ns() {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %%globaltimer;\n" : "=l"(t));
+  return t;
+}
+// bounded wait on a phase parity: false once 2 s of wall time have passed
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity) {
+  const uint32_t addr = smem_u32(bar);
+  const uint64_t t0 = globaltimer_ns();
+  while (true) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.b32 %0, 1, 0, p;\n\t}\n"
+        : "=r"(ok)
+        : "r"(addr), "r"(parity)
+        : "memory");
+    if (ok) return true;
+    if (globaltimer_ns() - t0 > 2000000000ull) return false;
+  }
+}
+__device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t bytes, uint64_t *bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(
+          smem_u32(dst)),
+      "l"(src), "r"(bytes), "r"(smem_u32(bar))
+      : "memory");
+}
+// K-major operand descriptor, no swizzle: 8-row × 16-byte core matrices, LBO between the
+// two K core matrices of one instruction, SBO between 8-row groups; version 1.
+__device__ __forceinline__ uint64_t umma_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+  uint64_t d = 0;
+  d |= (uint64_t)((saddr & 0x3FFFF) >> 4);
+  d |= (uint64_t)((lbo >> 4) & 0x3FFF) << 16;
+  d |= (uint64_t)((sbo >> 4) & 0x3FFF) << 32;
+  d |= (uint64_t)1 << 46;
+  return d;
+}
+__device__ __forceinline__ void umma_i8(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
+                                        uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(tmem_d),
+      "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate));
+}
+__device__ __forceinline__ void umma_commit(uint64_t *bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(
+                   smem_u32(bar))
+               : "memory");
+}
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&r)[16]) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, "
+      "[%16];\n"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+        "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+      : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+}
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory"); }
+
+constexpr uint32_t kTmemCols = 512;
+// instruction descriptor: D s32 (bits 4-5 = 2), A/B signed int8 (bits 7-9, 10-12 = 1),
+// both K-major, N = 64 (bits 17-22 = 64>>3), M = 128 (bits 24-28 = 128>>4)
+constexpr uint32_t kIdescI8 = (2u << 4) | (1u << 7) | (1u << 10) | ((64u >> 3) << 17) | ((128u >> 4) << 24);
+
+template <int S>
+__global__ void __launch_bounds__(128, 1)
+    gemm_split_tc_kernel(const GBlock *__restrict__ blocks, const GTile *__restrict__ tiles,
+                         const int8_t *__restrict__ ws, int cplx, double *__restrict__ C, CDbl alpha,
+                         CDbl beta, int *err) {
+  constexpr uint32_t A_BYTES = S * PANEL_A * KSTAGE, B_BYTES = S * PANEL_B * KSTAGE;
+  constexpr uint32_t STAGE = A_BYTES + B_BYTES;
+  extern __shared__ __align__(1024) unsigned char smem[];
+  uint64_t *full = reinterpret_cast<uint64_t *>(smem + 2 * STAGE);
+  uint64_t *empty = full + 2;
+  uint64_t *done = full + 4;
+  uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(full + 6);
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const GTile tile = tiles[blockIdx.x];
+  const GBlock b = blocks[tile.block];
+  const bool has_k = tile.kind == 0;
+  const int nk = has_k ? b.kpad / KSTAGE : 0;
+  const bool bz = beta.x == 0.0 && beta.y == 0.0;
+
+  if (tid == 0) {
+    mbar_init(&full[0], 1);
+    mbar_init(&full[1], 1);
+    mbar_init(&empty[0], 1);
+    mbar_init(&empty[1], 1);
+    mbar_init(done, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+  }
+  if (warp == 0 && has_k) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(smem_u32(tmem_slot)),
+                 "r"(kTmemCols));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::);
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = has_k ? *tmem_slot : 0u;
+
+  if (has_k && tid == 0) {
+    const int8_t *gA = ws + b.wsA + (int64_t)(tile.m0 / PANEL_A) * PANEL_A * b.kpad;
+    const int8_t *gB = ws + b.wsB + (int64_t)(tile.n0 / PANEL_B) * PANEL_B * b.kpad;
+    const int64_t planeA = (int64_t)b.mpad * b.kpad, planeB = (int64_t)b.npad * b.kpad;
+    auto load = [&](int kt, int st) {
+      unsigned char *sa = smem + st * STAGE;
+      mbar_expect_tx(&full[st], STAGE);
+#pragma unroll
+      for (int s = 0; s < S; ++s)
+        bulk_g2s(sa + s * (PANEL_A * KSTAGE), gA + s * planeA + (int64_t)kt * PANEL_A * KSTAGE,
+                 PANEL_A * KSTAGE, &full[st]);
+#pragma unroll
+      for (int s = 0; s < S; ++s)
+        bulk_g2s(sa + A_BYTES + s * (PANEL_B * KSTAGE), gB + s * planeB + (int64_t)kt * PANEL_B * KSTAGE,
+                 PANEL_B * KSTAGE, &full[st]);
+    };
+    bool ok = true;
+    int issued = 0, consumed = 0;  // stages loaded / waited on
+    load(0, 0);
+    issued = 1;
+    for (int kt = 0; kt < nk && ok; ++kt) {
+      const int st = kt & 1;
+      if (kt + 1 < nk) {
+        const int st2 = (kt + 1) & 1;
+        if (kt + 1 >= 2) ok = mbar_wait(&empty[st2], ((kt + 1) / 2 - 1) & 1);
+        if (!ok) break;
+        load(kt + 1, st2);
+        ++issued;
+      }
+      ok = mbar_wait(&full[st], (kt / 2) & 1);
+      if (!ok) break;
+      ++consumed;
+      tc_fence_after();
+      const uint32_t a0 = smem_u32(smem + st * STAGE), b0 = a0 + A_BYTES;
+#pragma unroll
+      for (int j = 0; j < KSTAGE / 32; ++j) {
+#pragma unroll
+        for (int s = 0; s < S; ++s) {
+          const uint64_t ad = umma_desc(a0 + s * (PANEL_A * KSTAGE) + j * 256, 128, 512);
+#pragma unroll
+          for (int t = 0; t < S - s; ++t) {
+            const uint64_t bd = umma_desc(b0 + t * (PANEL_B * KSTAGE) + j * 256, 128, 512);
+            const uint32_t acc = (kt > 0 || j > 0 || s > 0) ? 1u : 0u;
+            umma_i8(tmem + (uint32_t)((s + t) * 64), ad, bd, kIdescI8, acc);
+          }
+        }
+      }
+      umma_commit(&empty[st]);
+    }
+    umma_commit(done);
+    if (!ok) {
+      atomicExch(err, 1);
+      // let every bulk copy still in flight land before the CTA can exit (bounded)
+      for (int k = consumed; k < issued; ++k) mbar_wait(&full[k & 1], (k / 2) & 1);
+    }
+  }
+  if (has_k) {
+    if (!mbar_wait(done, 0)) atomicExch(err, 2);
+    tc_fence_after();
+  }
+  __syncwarp();  // tcgen05.ld is warp-collective: reconverge after the divergent waits
+  // epilogue: warp w owns accumulator rows 32w..32w+31 (TMEM lanes)
+  const int32_t *eA = reinterpret_cast<const int32_t *>(ws + b.wsEA);
+  const int32_t *eB = reinterpret_cast<const int32_t *>(ws + b.wsEB);
+  const int64_t Mreal = cplx ? 2 * b.m : b.m;
+  const int64_t i = tile.m0 + 32 * warp + lane;
+  const int ei = (has_k && i < Mreal) ? eA[i] : 0;
+#pragma unroll 1
+  for (int c = 0; c < 4; ++c) {
+    double v[16];
+#pragma unroll
+    for (int q = 0; q < 16; ++q) v[q] = 0.0;
+    if (has_k) {
+#pragma unroll
+      for (int d = S - 1; d >= 0; --d) {
+        uint32_t r[16];
+        tmem_ld16(tmem + ((uint32_t)(32 * warp) << 16) + (uint32_t)(d * 64 + c * 16), r);
+#pragma unroll
+        for (int q = 0; q < 16; ++q) v[q] += ldexp((double)(int32_t)r[q], -7 * (d + 2));
       }
     }
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
-    int e = 0;
-    if (mx > 0.0) frexp(mx, &e);  // mx < 2^e
-    if (lane == 0) expo[r] = e;
-    for (int64_t l = lane; l < kpad; l += 32) {
-      double x = 0.0;
-      if (valid && l < Klog) x = ldexp(op_elem(b, job.operand, cplx, X, r, l), -e);
-      for (int s = 0; s < S; ++s) {
-        x *= 128.0;
-        const double q = trunc(x);
-        x -= q;
-        base[(int64_t)s * rows_pad * kpad + r * kpad + l] = (int8_t)q;
-      }
+    for (int q = 0; q < 16; ++q) {
+      const int64_t j = tile.n0 + c * 16 + q;
+      double val = v[q];
+      if (has_k) val = ldexp(val, ei + ((j < b.n) ? eB[j] : 0));
+      store_out(val, i, j, b, cplx, C, alpha, beta, bz, 1);
     }
-    (void)rows_pad;
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 0 && has_k) {
+    tc_fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(kTmemCols));
   }
 }
+
+// ---- mma.sync product kernel (comparison path) -------------------------------------------------
+constexpr int SBM = 64, SBN = 64, SBK = 32;
+constexpr int SPITCH = 48;  // smem row pitch in bytes: conflict-free fragment loads
 
 __device__ __forceinline__ void cp_async16(void *smem, const void *gmem) {
   const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
@@ -141,19 +474,19 @@ __device__ __forceinline__ void imma(int (&c)[4], const int (&a)[4], const int (
 }
 
 template <int S>
-__device__ __forceinline__ void load_stage(int8_t *As, int8_t *Bs, const GBlock &b,
-                                           const int8_t *ws, int64_t m0, int64_t n0, int64_t k0) {
-  // per slice: 64 rows x 32 bytes = 128 chunks of 16 bytes for each operand
+__device__ __forceinline__ void load_stage(int8_t *As, int8_t *Bs, const GBlock &b, const int8_t *ws,
+                                           int64_t m0, int64_t n0, int64_t k0) {
+  const int64_t planeA = (int64_t)b.mpad * b.kpad, planeB = (int64_t)b.npad * b.kpad;
   for (int c = threadIdx.x; c < 2 * S * 128; c += blockDim.x) {
     const int op = c / (S * 128);
     const int rem = c % (S * 128);
     const int s = rem / 128, q = rem % 128;
     const int row = q >> 1, half = q & 1;
     if (op == 0) {
-      const int8_t *g = ws + b.wsA + ((int64_t)s * b.mpad + m0 + row) * b.kpad + k0 + half * 16;
+      const int8_t *g = ws + b.wsA + s * planeA + slice_off(m0 + row, k0 + half * 16, b.kpad, PANEL_A);
       cp_async16(As + (s * SBM + row) * SPITCH + half * 16, g);
     } else {
-      const int8_t *g = ws + b.wsB + ((int64_t)s * b.npad + n0 + row) * b.kpad + k0 + half * 16;
+      const int8_t *g = ws + b.wsB + s * planeB + slice_off(n0 + row, k0 + half * 16, b.kpad, PANEL_B);
       cp_async16(Bs + (s * SBN + row) * SPITCH + half * 16, g);
     }
   }
@@ -180,109 +513,85 @@ __global__ void __launch_bounds__(256)
     if (ti >= ntiles) break;
     const GTile tile = tiles[ti];
     const GBlock b = blocks[tile.block];
-    const int64_t m0 = tile.m0, n0 = tile.n0;
-    int acc[S][2][2][4];
+    // mma.sync tiles are 64 x 64 quarters of the 128 x 64 tcgen05 tiles
+    for (int half = 0; half < 2; ++half) {
+      const int64_t m0 = tile.m0 + half * 64, n0 = tile.n0;
+      int acc[S][2][2][4];
 #pragma unroll
-    for (int d = 0; d < S; ++d)
+      for (int d = 0; d < S; ++d)
+#pragma unroll
+        for (int mt = 0; mt < 2; ++mt)
+#pragma unroll
+          for (int nt = 0; nt < 2; ++nt)
+#pragma unroll
+            for (int q = 0; q < 4; ++q) acc[d][mt][nt][q] = 0;
+      const int64_t nk = b.kpad / SBK;
+      if (tile.kind == 0 && nk > 0) {
+        load_stage<S>(As0, As0 + S * SBM * SPITCH, b, ws, m0, n0, 0);
+        cp_commit();
+        for (int64_t kt = 0; kt < nk; ++kt) {
+          int8_t *As = As0 + (kt & 1) * stage_bytes;
+          int8_t *Bs = As + S * SBM * SPITCH;
+          if (kt + 1 < nk) {
+            int8_t *An = As0 + ((kt + 1) & 1) * stage_bytes;
+            load_stage<S>(An, An + S * SBM * SPITCH, b, ws, m0, n0, (kt + 1) * SBK);
+            cp_commit();
+            cp_wait1();
+          } else {
+            cp_wait0();
+          }
+          __syncthreads();
+#pragma unroll
+          for (int s = 0; s < S; ++s) {
+            int af[2][4];
+#pragma unroll
+            for (int mt = 0; mt < 2; ++mt) {
+              const int8_t *p = As + (s * SBM + wm * 32 + mt * 16 + g) * SPITCH + tig * 4;
+              af[mt][0] = *reinterpret_cast<const int *>(p);
+              af[mt][1] = *reinterpret_cast<const int *>(p + 8 * SPITCH);
+              af[mt][2] = *reinterpret_cast<const int *>(p + 16);
+              af[mt][3] = *reinterpret_cast<const int *>(p + 8 * SPITCH + 16);
+            }
+#pragma unroll
+            for (int t = 0; t < S - s; ++t) {
+              int bf[2][2];
+#pragma unroll
+              for (int nt = 0; nt < 2; ++nt) {
+                const int8_t *p = Bs + (t * SBN + wn * 16 + nt * 8 + g) * SPITCH + tig * 4;
+                bf[nt][0] = *reinterpret_cast<const int *>(p);
+                bf[nt][1] = *reinterpret_cast<const int *>(p + 16);
+              }
+#pragma unroll
+              for (int mt = 0; mt < 2; ++mt)
+#pragma unroll
+                for (int nt = 0; nt < 2; ++nt) imma(acc[s + t][mt][nt], af[mt], bf[nt]);
+            }
+          }
+          __syncthreads();
+        }
+      }
+      const int32_t *eA = reinterpret_cast<const int32_t *>(ws + b.wsEA);
+      const int32_t *eB = reinterpret_cast<const int32_t *>(ws + b.wsEB);
+      const int64_t Mreal = cplx ? 2 * b.m : b.m;
 #pragma unroll
       for (int mt = 0; mt < 2; ++mt)
 #pragma unroll
-        for (int nt = 0; nt < 2; ++nt)
+        for (int hr = 0; hr < 2; ++hr) {
+          const int64_t i = m0 + wm * 32 + mt * 16 + g + hr * 8;
 #pragma unroll
-          for (int q = 0; q < 4; ++q) acc[d][mt][nt][q] = 0;
-    const int64_t nk = b.kpad / SBK;
-    if (tile.kind == 0 && nk > 0) {
-      load_stage<S>(As0, As0 + S * SBM * SPITCH, b, ws, m0, n0, 0);
-      cp_commit();
-      for (int64_t kt = 0; kt < nk; ++kt) {
-        int8_t *As = As0 + (kt & 1) * stage_bytes;
-        int8_t *Bs = As + S * SBM * SPITCH;
-        if (kt + 1 < nk) {
-          int8_t *An = As0 + ((kt + 1) & 1) * stage_bytes;
-          load_stage<S>(An, An + S * SBM * SPITCH, b, ws, m0, n0, (kt + 1) * SBK);
-          cp_commit();
-          cp_wait1();
-        } else {
-          cp_wait0();
-        }
-        __syncthreads();
+          for (int nt = 0; nt < 2; ++nt)
 #pragma unroll
-        for (int s = 0; s < S; ++s) {
-          int af[2][4];
+            for (int hc = 0; hc < 2; ++hc) {
+              const int64_t j = n0 + wn * 16 + nt * 8 + 2 * tig + hc;
+              double v = 0.0;
+              if (tile.kind == 0) {
 #pragma unroll
-          for (int mt = 0; mt < 2; ++mt) {
-            const int8_t *p = As + (s * SBM + wm * 32 + mt * 16 + g) * SPITCH + tig * 4;
-            af[mt][0] = *reinterpret_cast<const int *>(p);
-            af[mt][1] = *reinterpret_cast<const int *>(p + 8 * SPITCH);
-            af[mt][2] = *reinterpret_cast<const int *>(p + 16);
-            af[mt][3] = *reinterpret_cast<const int *>(p + 8 * SPITCH + 16);
-          }
-#pragma unroll
-          for (int t = 0; t < S - s; ++t) {
-            int bf[2][2];
-#pragma unroll
-            for (int nt = 0; nt < 2; ++nt) {
-              const int8_t *p = Bs + (t * SBN + wn * 16 + nt * 8 + g) * SPITCH + tig * 4;
-              bf[nt][0] = *reinterpret_cast<const int *>(p);
-              bf[nt][1] = *reinterpret_cast<const int *>(p + 16);
-            }
-#pragma unroll
-            for (int mt = 0; mt < 2; ++mt)
-#pragma unroll
-              for (int nt = 0; nt < 2; ++nt) imma(acc[s + t][mt][nt], af[mt], bf[nt]);
-          }
-        }
-        __syncthreads();
-      }
-    }
-    // epilogue: recombine the diagonals in FP64, smallest weight first
-    const int32_t *eA = reinterpret_cast<const int32_t *>(ws + b.wsEA);
-    const int32_t *eB = reinterpret_cast<const int32_t *>(ws + b.wsEB);
-    const int64_t Mreal = cplx ? 2 * b.m : b.m;
-#pragma unroll
-    for (int mt = 0; mt < 2; ++mt) {
-#pragma unroll
-      for (int hr = 0; hr < 2; ++hr) {
-        const int64_t i = m0 + wm * 32 + mt * 16 + g + hr * 8;
-#pragma unroll
-        for (int nt = 0; nt < 2; ++nt) {
-#pragma unroll
-          for (int hc = 0; hc < 2; ++hc) {
-            const int64_t j = n0 + wn * 16 + nt * 8 + 2 * tig + hc;
-            double v = 0.0;
-            if (tile.kind == 0) {
-#pragma unroll
-              for (int d = S - 1; d >= 0; --d)
-                v += ldexp((double)acc[d][mt][nt][hr * 2 + hc], -7 * (d + 2));
-              const int ei = (i < Mreal) ? eA[i] : 0;
-              const int ej = (j < b.n) ? eB[j] : 0;
-              v = ldexp(v, ei + ej);
-            }
-            if (!cplx) {
-              if (i < b.m && j < b.n) {
-                double *p = C + b.offC + i + j * b.ldc;
-                double r = alpha.x * v;
-                if (!bz) r = fma(beta.x, *p, r);
-                *p = r;
+                for (int d = S - 1; d >= 0; --d) v += ldexp((double)acc[d][mt][nt][hr * 2 + hc], -7 * (d + 2));
+                v = ldexp(v, ((i < Mreal) ? eA[i] : 0) + ((j < b.n) ? eB[j] : 0));
               }
-            } else {
-              const double w = __shfl_xor_sync(0xffffffffu, v, 4);  // partner row (g ^ 1)
-              if (!(g & 1) && i < Mreal && j < b.n) {
-                const double vr = v, vi = w;
-                double2 *p = reinterpret_cast<double2 *>(C) + b.offC + (i >> 1) + j * b.ldc;
-                double rr = alpha.x * vr - alpha.y * vi;
-                double ri = alpha.x * vi + alpha.y * vr;
-                if (!bz) {
-                  const double2 o = *p;
-                  rr = fma(beta.x, o.x, fma(-beta.y, o.y, rr));
-                  ri = fma(beta.x, o.y, fma(beta.y, o.x, ri));
-                }
-                *p = make_double2(rr, ri);
-              }
+              store_out(v, i, j, b, cplx, C, alpha, beta, bz, 4);
             }
-          }
         }
-      }
     }
   }
   if (threadIdx.x == 0) {
@@ -296,16 +605,39 @@ __global__ void __launch_bounds__(256)
   }
 }
 
+bool use_mma_sync() {
+  const char *e = std::getenv("TKB_SPLIT_KERNEL");
+  return e && std::strcmp(e, "mma") == 0;
+}
+
 template <int S>
-int launch_split(tkb_ctx *ctx, const tkb_plan *p, void *C, CDbl a, CDbl b) {
-  const size_t smem = 2 * (size_t)(2 * S * SBM * SPITCH);
-  auto k = gemm_split_mma_kernel<S>;
-  TKB_CUDA_TRY(ctx, cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  const int grid = (int)std::min<int64_t>(p->nstiles, (int64_t)ctx->num_sms * 2);
-  k<<<grid, 256, smem, ctx->stream>>>(p->blocks, p->stiles, (int)p->nstiles, ctx->counters,
-                                      (const int8_t *)ctx->ws, p->dtype == TKB_C128 ? 1 : 0,
-                                      (double *)C, a, b);
+int launch_split(tkb_ctx *ctx, const tkb_plan *p, void *C, const void *A, const void *B, CDbl a, CDbl b) {
+  const int cplx = p->dtype == TKB_C128 ? 1 : 0;
+  if (p->nsrows > 0) {
+    // one CTA per 32-row group
+    const int grid = (int)std::min<int64_t>(p->nsrows, (int64_t)ctx->num_sms * 8);
+    slice_kernel<S><<<grid, 256, 0, ctx->stream>>>(p->blocks, p->srow_begin, (const SliceJob *)p->sjobs,
+                                                   p->nsjobs, p->nsrows, cplx, (const double *)A,
+                                                   (const double *)B, (int8_t *)ctx->ws);
+    ctx->launches++;
+    TKB_CUDA_TRY(ctx, cudaGetLastError());
+  }
+  if (use_mma_sync()) {
+    const size_t smem = 2 * (size_t)(2 * S * SBM * SPITCH);
+    auto k = gemm_split_mma_kernel<S>;
+    TKB_CUDA_TRY(ctx, cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    const int grid = (int)std::min<int64_t>(p->nstiles, (int64_t)ctx->num_sms * 2);
+    k<<<grid, 256, smem, ctx->stream>>>(p->blocks, p->stiles, (int)p->nstiles, ctx->counters,
+                                        (const int8_t *)ctx->ws, cplx, (double *)C, a, b);
+  } else {
+    const size_t smem = 2 * (size_t)S * (PANEL_A + PANEL_B) * KSTAGE + 64;
+    auto k = gemm_split_tc_kernel<S>;
+    TKB_CUDA_TRY(ctx, cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    k<<<(int)p->nstiles, 128, smem, ctx->stream>>>(p->blocks, p->stiles, (const int8_t *)ctx->ws, cplx,
+                                                   (double *)C, a, b, ctx->counters + 8);
+  }
   ctx->launches++;
+  TKB_CUDA_TRY(ctx, cudaGetLastError());
   return TKB_OK;
 }
 
@@ -321,17 +653,17 @@ int tkb_gemm_split_prepare(tkb_ctx *ctx, tkb_plan *p) {
   p->slices = S;
   size_t off = 0;
   std::vector<SliceJob> jobs;
-  std::vector<int64_t> row_begin;
+  std::vector<int64_t> grp_begin;
   std::vector<GTile> tiles;
-  int64_t nrows = 0;
+  int64_t ngroups = 0;
   for (size_t bi = 0; bi < p->hblocks.size(); ++bi) {
     GBlock &b = p->hblocks[bi];
     const int64_t M = cplx ? 2 * b.m : b.m;
     const int64_t K = cplx ? 2 * b.k : b.k;
-    b.mpad = (int32_t)roundup(std::max<int64_t>(M, 1), SBM);
-    b.npad = (int32_t)roundup(std::max<int64_t>(b.n, 1), SBN);
-    b.kpad = (int32_t)roundup(std::max<int64_t>(K, 1), SBK);
-    if (b.m == 0 || b.n == 0) continue;
+    b.mpad = (int32_t)roundup(std::max<int64_t>(M, 1), PANEL_A);
+    b.npad = (int32_t)roundup(std::max<int64_t>(b.n, 1), PANEL_B);
+    b.kpad = (int32_t)roundup(std::max<int64_t>(K, 1), KSTAGE);
+    if (b.m == 0 || b.n == 0 || b.skinny) continue;
     b.wsA = (int64_t)off;
     off += (size_t)S * b.mpad * b.kpad;
     b.wsB = (int64_t)off;
@@ -345,14 +677,14 @@ int tkb_gemm_split_prepare(tkb_ctx *ctx, tkb_plan *p) {
     const int kind = b.k > 0 ? 0 : 1;
     if (kind == 0) {
       jobs.push_back({(int32_t)bi, 0});
-      row_begin.push_back(nrows);
-      nrows += b.mpad;
+      grp_begin.push_back(ngroups);
+      ngroups += b.mpad / 32;
       jobs.push_back({(int32_t)bi, 1});
-      row_begin.push_back(nrows);
-      nrows += b.npad;
+      grp_begin.push_back(ngroups);
+      ngroups += b.npad / 32;
     }
-    for (int64_t m0 = 0; m0 < M; m0 += SBM)
-      for (int64_t n0 = 0; n0 < b.n; n0 += SBN) tiles.push_back({(int32_t)bi, (int32_t)m0, (int32_t)n0, kind});
+    for (int64_t m0 = 0; m0 < M; m0 += PANEL_A)
+      for (int64_t n0 = 0; n0 < b.n; n0 += PANEL_B) tiles.push_back({(int32_t)bi, (int32_t)m0, (int32_t)n0, kind});
   }
   std::stable_sort(tiles.begin(), tiles.end(), [&](const GTile &x, const GTile &y) {
     return p->hblocks[x.block].kpad > p->hblocks[y.block].kpad;
@@ -360,7 +692,7 @@ int tkb_gemm_split_prepare(tkb_ctx *ctx, tkb_plan *p) {
   p->ws_bytes = off;
   p->nstiles = (int64_t)tiles.size();
   p->nsjobs = (int)jobs.size();
-  p->nsrows = nrows;
+  p->nsrows = ngroups;
   cudaError_t e = cudaSuccess;
   if (!tiles.empty()) {
     e = cudaMalloc((void **)&p->stiles, tiles.size() * sizeof(GTile));
@@ -369,8 +701,8 @@ int tkb_gemm_split_prepare(tkb_ctx *ctx, tkb_plan *p) {
   if (e == cudaSuccess && !jobs.empty()) {
     e = cudaMalloc(&p->sjobs, jobs.size() * sizeof(SliceJob));
     if (e == cudaSuccess) e = cudaMemcpy(p->sjobs, jobs.data(), jobs.size() * sizeof(SliceJob), cudaMemcpyHostToDevice);
-    if (e == cudaSuccess) e = cudaMalloc((void **)&p->srow_begin, row_begin.size() * 8);
-    if (e == cudaSuccess) e = cudaMemcpy(p->srow_begin, row_begin.data(), row_begin.size() * 8, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMalloc((void **)&p->srow_begin, grp_begin.size() * 8);
+    if (e == cudaSuccess) e = cudaMemcpy(p->srow_begin, grp_begin.data(), grp_begin.size() * 8, cudaMemcpyHostToDevice);
   }
   if (e != cudaSuccess)
     return tkb_set_error(ctx, TKB_ERR_CUDA, std::string("split plan upload: ") + cudaGetErrorString(e));
@@ -384,27 +716,12 @@ int tkb_gemm_split_launch(tkb_ctx *ctx, const tkb_plan *p, void *C, const void *
     return tkb_set_error(ctx, TKB_ERR_ARG, "complex scalar with real data");
   if (ctx->ws_bytes < p->ws_bytes)
     return tkb_set_error(ctx, TKB_ERR_ARG, "context workspace smaller than the plan needs");
-  const int cplx = p->dtype == TKB_C128 ? 1 : 0;
-  if (p->nsrows > 0) {
-    const int64_t warps = p->nsrows;
-    const int grid = (int)std::min<int64_t>((warps + 7) / 8, (int64_t)ctx->num_sms * 16);
-    slice_kernel<<<grid, 256, 0, ctx->stream>>>(p->blocks, p->srow_begin,
-                                                (const SliceJob *)p->sjobs, p->nsjobs, p->nsrows,
-                                                p->slices, cplx, (const double *)A,
-                                                (const double *)B, (int8_t *)ctx->ws);
-    ctx->launches++;
-    TKB_CUDA_TRY(ctx, cudaGetLastError());
-  }
   CDbl a{alpha.re, alpha.im}, b{beta.re, beta.im};
-  int rc;
   switch (p->slices) {
-    case 3: rc = launch_split<3>(ctx, p, C, a, b); break;
-    case 4: rc = launch_split<4>(ctx, p, C, a, b); break;
-    case 5: rc = launch_split<5>(ctx, p, C, a, b); break;
-    case 6: rc = launch_split<6>(ctx, p, C, a, b); break;
-    default: rc = launch_split<7>(ctx, p, C, a, b); break;
+    case 3: return launch_split<3>(ctx, p, C, A, B, a, b);
+    case 4: return launch_split<4>(ctx, p, C, A, B, a, b);
+    case 5: return launch_split<5>(ctx, p, C, A, B, a, b);
+    case 6: return launch_split<6>(ctx, p, C, A, B, a, b);
+    default: return launch_split<7>(ctx, p, C, A, B, a, b);
   }
-  if (rc != TKB_OK) return rc;
-  TKB_CUDA_TRY(ctx, cudaGetLastError());
-  return TKB_OK;
 }

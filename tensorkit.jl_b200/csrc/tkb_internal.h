@@ -79,8 +79,14 @@ struct GBlock {
   // split precision: workspace offsets of the sliced operands and exponents
   int64_t wsA, wsB, wsEA, wsEB;
   int32_t mpad, npad, kpad;   // padded extents (tile multiples) of the sliced operands
-  int32_t pad_;
+  int32_t skinny;             // 1: n, k ≤ 16 — memory-bound row kernel in every precision
 };
+
+constexpr int kSkinnyMax = 16;  // n and k bound of the skinny (row-per-thread) path
+constexpr int kSkinnyRows = 256;
+
+int tkb_gemm_skinny_launch(tkb_ctx *ctx, const tkb_plan *p, void *C, const void *A,
+                           const void *B, tkb_scalar alpha, tkb_scalar beta);
 
 struct GTile {
   int32_t block;
@@ -92,6 +98,8 @@ struct tkb_plan {
   tkb_ctx *owner = nullptr;
   int dtype = 0, precision = 0, slices = 0;
   int64_t nblocks = 0, ntiles = 0;
+  GTile *sktasks = nullptr;     // skinny blocks: (block, first row) tasks of kSkinnyRows rows
+  int64_t nsk = 0;
   double flops = 0;
   int64_t lenA = 0, lenB = 0, lenC = 0;
   std::vector<GBlock> hblocks;

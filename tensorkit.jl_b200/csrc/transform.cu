@@ -25,6 +25,8 @@
 namespace {
 
 constexpr int kThreads = 256;
+constexpr int kBatch = 8;  // elements per thread per load batch (loads in flight per thread)
+constexpr int64_t kTileElemsMax = 2048;  // largest task (= kThreads * kBatch elements)
 constexpr size_t kSmemBudget = 96 * 1024;
 
 struct CDbl {
@@ -128,6 +130,13 @@ __global__ void __launch_bounds__(kThreads)
       return off;
     };
 
+    // Tile extents are powers of two: index decomposition by shifts and masks, elements
+    // outside the (na, nb) corner are skipped. Every thread issues its loads of a batch of
+    // kBatch elements before using any of them, so each thread keeps kBatch loads in flight.
+    const int lta = __ffs(ta) - 1, ltb = __ffs(tb) - 1;
+    const int tot = ta * tb;
+    (void)nel;
+
     if (G.mode == 0 && nsrc == 1 && ndst == 1) {
       // direct copy: coalesced along a on both sides
       const int64_t *ss = sstr + G.src_tree_begin * TKB_MAX_IND;
@@ -136,12 +145,24 @@ __global__ void __launch_bounds__(kThreads)
       const int64_t sB = db >= 0 ? ss[db] : 0, dB = db >= 0 ? ds[db] : 0;
       const int64_t sb0 = src_base(0), db0 = dst_base(0);
       const double u = coeffs[G.coeff_begin];
-      for (int e = threadIdx.x; e < nel; e += kThreads) {
-        const int ia = e % na, ib = e / na;
-        T v = ld_val(src + sb0 + ia * sA + ib * sB, CONJ);
-        T acc = axpy_r(u, v, zero_val(v));
-        T *dp = dst + db0 + ia * dA + ib * dB;
-        *dp = finish(acc, alpha, beta, dp, bz);
+      for (int e0 = 0; e0 < tot; e0 += kThreads * kBatch) {
+        T v[kBatch];
+#pragma unroll
+        for (int q = 0; q < kBatch; ++q) {
+          const int e = e0 + q * kThreads + threadIdx.x;
+          const int ia = e & (ta - 1), ib = e >> lta;
+          v[q] = (e < tot && ia < na && ib < nb) ? ld_val(src + sb0 + ia * sA + ib * sB, CONJ)
+                                                : zero_val(T{});
+        }
+#pragma unroll
+        for (int q = 0; q < kBatch; ++q) {
+          const int e = e0 + q * kThreads + threadIdx.x;
+          const int ia = e & (ta - 1), ib = e >> lta;
+          if (e < tot && ia < na && ib < nb) {
+            T *dp = dst + db0 + ia * dA + ib * dB;
+            *dp = finish(axpy_r(u, v[q], zero_val(T{})), alpha, beta, dp, bz);
+          }
+        }
       }
       continue;
     }
@@ -154,15 +175,23 @@ __global__ void __launch_bounds__(kThreads)
       const int64_t sA = ss[da], sB = db >= 0 ? ss[db] : 0;
       const int64_t base = src_base(j);
       T *tile = sm + j * tile_elems;
-      if (G.mode == 1) {
-        for (int e = threadIdx.x; e < nel; e += kThreads) {
-          const int ib = e % nb, ia = e / nb;  // b fastest: coalesced source reads
-          tile[ia * pitch + ib] = ld_val(src + base + ia * sA + ib * sB, CONJ);
+      for (int e0 = 0; e0 < tot; e0 += kThreads * kBatch) {
+        T v[kBatch];
+#pragma unroll
+        for (int q = 0; q < kBatch; ++q) {
+          const int e = e0 + q * kThreads + threadIdx.x;
+          // transpose mode: b fastest (coalesced source reads); copy mode: a fastest
+          const int ia = G.mode == 1 ? (e >> ltb) : (e & (ta - 1));
+          const int ib = G.mode == 1 ? (e & (tb - 1)) : (e >> lta);
+          v[q] = (e < tot && ia < na && ib < nb) ? ld_val(src + base + ia * sA + ib * sB, CONJ)
+                                                : zero_val(T{});
         }
-      } else {
-        for (int e = threadIdx.x; e < nel; e += kThreads) {
-          const int ia = e % na, ib = e / na;
-          tile[ib * ta + ia] = ld_val(src + base + ia * sA + ib * sB, CONJ);
+#pragma unroll
+        for (int q = 0; q < kBatch; ++q) {
+          const int e = e0 + q * kThreads + threadIdx.x;
+          const int ia = G.mode == 1 ? (e >> ltb) : (e & (ta - 1));
+          const int ib = G.mode == 1 ? (e & (tb - 1)) : (e >> lta);
+          if (e < tot) tile[G.mode == 1 ? ia * pitch + ib : ib * ta + ia] = v[q];
         }
       }
     }
@@ -173,13 +202,19 @@ __global__ void __launch_bounds__(kThreads)
       const int64_t dA = ds[da], dB = db >= 0 ? ds[db] : 0;
       const int64_t base = dst_base(i);
       const double *Ui = U + i * nsrc;
-      for (int e = threadIdx.x; e < nel; e += kThreads) {
-        const int ia = e % na, ib = e / na;  // a fastest: coalesced destination writes
-        const int sidx = (G.mode == 1) ? ia * pitch + ib : ib * ta + ia;
-        T acc = zero_val(T{});
-        for (int64_t j = 0; j < nsrc; ++j) acc = axpy_r(Ui[j], sm[j * tile_elems + sidx], acc);
-        T *dp = dst + base + ia * dA + ib * dB;
-        *dp = finish(acc, alpha, beta, dp, bz);
+      for (int e0 = 0; e0 < tot; e0 += kThreads * kBatch) {
+#pragma unroll
+        for (int q = 0; q < kBatch; ++q) {
+          const int e = e0 + q * kThreads + threadIdx.x;
+          const int ia = e & (ta - 1), ib = e >> lta;  // a fastest: coalesced destination writes
+          if (e < tot && ia < na && ib < nb) {
+            const int sidx = (G.mode == 1) ? ia * pitch + ib : ib * ta + ia;
+            T acc = zero_val(T{});
+            for (int64_t j = 0; j < nsrc; ++j) acc = axpy_r(Ui[j], sm[j * tile_elems + sidx], acc);
+            T *dp = dst + base + ia * dA + ib * dB;
+            *dp = finish(acc, alpha, beta, dp, bz);
+          }
+        }
       }
     }
     __syncthreads();
@@ -220,6 +255,18 @@ extern "C" int tkb_table_create(tkb_ctx *ctx, const tkb_table_desc *d, tkb_table
   int64_t ntasks = 0, er = 0, ew = 0;
   size_t smem_max_f64 = 0, smem_max_c128 = 0;
   int max_trees = 1;
+  // tile target: 2048 elements per task, smaller when the whole transform would not give
+  // every SM about four tasks (small permutes are latency-bound, not bandwidth-bound)
+  int64_t kTileElems = kTileElemsMax;
+  {
+    int64_t total = 0;
+    for (int64_t g = 0; g < G; ++g) {
+      int64_t vol = 1;
+      for (int k = 0; k < N; ++k) vol *= std::max<int64_t>(1, d->sizes[g * N + k]);
+      total += vol * (d->group_dst_ptr[g + 1] - d->group_dst_ptr[g]);
+    }
+    while (kTileElems > 256 && total / kTileElems < (int64_t)ctx->num_sms * 4) kTileElems >>= 1;
+  }
 
   for (int64_t g = 0; g < G; ++g) {
     const int64_t s0 = d->group_src_ptr[g], s1 = d->group_src_ptr[g + 1];
@@ -317,8 +364,8 @@ extern "C" int tkb_table_create(tkb_ctx *ctx, const tkb_table_desc *d, tkb_table
       int64_t best = 0;
       for (int k = 0; k < nd; ++k)
         if (k != fa && dims[k].size > best) { best = dims[k].size; db = k; }
-      ta = std::min<int64_t>(pow2ceil(dims[fa].size), 1024);
-      tb = db >= 0 ? std::min<int64_t>(pow2ceil(dims[db].size), std::max<int64_t>(1, 1024 / ta)) : 1;
+      ta = std::min<int64_t>(pow2ceil(dims[fa].size), kTileElems);
+      tb = db >= 0 ? std::min<int64_t>(pow2ceil(dims[db].size), std::max<int64_t>(1, kTileElems / ta)) : 1;
       // shared-memory budget when several trees are staged
       while (nsrc > 1 && (size_t)(nsrc * ta * tb) * el128 > kSmemBudget && (ta > 1 || tb > 1)) {
         if (tb > 1) tb >>= 1; else ta >>= 1;
@@ -328,7 +375,7 @@ extern "C" int tkb_table_create(tkb_ctx *ctx, const tkb_table_desc *d, tkb_table
       db = fs;
       ta = std::min<int64_t>(pow2ceil(dims[fa].size), 32);
       tb = std::min<int64_t>(pow2ceil(dims[db].size), 32);
-      while (ta * tb < 1024) {
+      while (ta * tb < kTileElems) {
         const bool grow_a = ta < dims[fa].size && (ta <= tb || tb >= dims[db].size);
         const bool grow_b = tb < dims[db].size;
         if (grow_a && ta < 256) ta <<= 1;

@@ -32,6 +32,25 @@ def to_hom(W: O.Hom):
                        tk.ProductSpace([to_space(s) for s in W.dom], u), u)
 
 
+def from_sector(s):
+    from tensorkit_b200 import sectors as S
+    if isinstance(s, S.U1Irrep):
+        return ("U1", s.q2)
+    if isinstance(s, S.SU2Irrep):
+        return ("SU2", s.j2)
+    return ("P", tuple(from_sector(x) for x in s.sectors))
+
+
+def from_space(sp):
+    degs = {from_sector(c.dual() if sp.isdual() else c): sp.dim(c) for c in sp.sectors()}
+    return O.Space(degs, sp.isdual())
+
+
+def from_hom(W):
+    return O.Hom([from_space(v) for v in W.codomain], [from_space(v) for v in W.domain],
+                 from_sector(W.unit()))
+
+
 def to_device(t: O.BT, device="cuda"):
     import torch
     return tk.TensorMap(torch.from_numpy(np.ascontiguousarray(t.data)).to(device), to_hom(t.W))

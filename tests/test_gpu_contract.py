@@ -31,6 +31,35 @@ def test_cfg1_u1_small():
     assert relerr(Cp.to_host(), refp.data) <= TOL
 
 
+@pytest.mark.parametrize("prec", ["plain", "split"])
+def test_u1_two_site_heff(prec):
+    """y[a,p,q;b] := L[a,w;c]*x[c,r,s;d]*W1[w,p;r,v]*W2[v,q;s,u]*R[d,u;b] — many uneven
+    blocks, tall-skinny GEMMs against the MPO bond, four pairwise steps; also replayed
+    as a CUDA graph."""
+    from helpers import cfg3_spaces
+    V, Pp, Wm = cfg3_spaces()
+    Wd = Wm.flipdual()
+    tens = {"L": O.randn(O.Hom([V, Wd], [V]), 2), "x": O.randn(O.Hom([V, Pp, Pp], [V]), 2),
+            "W1": O.randn(O.Hom([Wm, Pp], [Pp, Wm]), 2), "W2": O.randn(O.Hom([Wm, Pp], [Pp, Wm]), 2),
+            "R": O.randn(O.Hom([V, Wm], [V]), 2)}
+    expr = "y[a,p,q;b] := L[a,w;c]*x[c,r,s;d]*W1[w,p;r,v]*W2[v,q;s,u]*R[d,u;b]"
+    from tensorkit_b200.tensoroperations import parse_tensor_expr
+    _, lhs, _, factors = parse_tensor_expr(expr)
+    ref = O.network(factors, lhs, tens)
+    dev = {k: to_device(v) for k, v in tens.items()}
+    plan = tk.NetworkPlan(expr, precision=prec, **dev).capture()
+    y = plan.replay()
+    plan.ctx.synchronize()
+    assert y.space == to_hom(ref.W)
+    assert relerr(y.to_host(), ref.data) <= TOL
+    # a second replay after changing an input in place
+    dev["x"].data.mul_(2.0)
+    y = plan.replay()
+    plan.ctx.synchronize()
+    assert relerr(y.to_host(), 2.0 * ref.data) <= TOL
+    plan.free()
+
+
 @pytest.mark.parametrize("mult,prec,cplx", [(1, "plain", False), (1, "split", False),
                                             (8, "plain", False), (8, "split", False),
                                             (8, "plain", True), (8, "split", True)])
