@@ -225,6 +225,9 @@ int tkb_gemm_plan_destroy(tkb_plan *p) {
   cudaFree(p->blocks);
   cudaFree(p->tiles);
   cudaFree(p->sktasks);
+  cudaFree(p->kstiles);
+  cudaFree(p->part);
+  cudaFree(p->pcnt);
   cudaFree(p->stiles);
   cudaFree(p->sjobs);
   cudaFree(p->srow_begin);

@@ -16,18 +16,19 @@
 // [Re B; Im B], so rows 2r and 2r+1 of the real result are Re and Im of C_r.
 //
 // Slice layout in the workspace: per block, per slice, the rows of op(A) (op(B)ᵀ) are cut
-// into panels of 128 (64) rows; a panel is a sequence of 64-byte K stages, each stored as
-// the canonical K-major "core matrix" layout of the tensor-core operand descriptors
-// (8-row × 16-byte core matrices; 512 bytes between 8-row groups, 128 bytes between the
-// four 16-byte K chunks). One stage of one slice is therefore one contiguous 8 KiB (4 KiB)
-// block that a single bulk copy moves into shared memory.
+// into panels of 128 (64) rows; a panel is a sequence of 32-byte K stages (one tensor-core
+// K step), each stored as the canonical K-major "core matrix" layout of the tensor-core
+// operand descriptors (8-row × 16-byte core matrices; 256 bytes between 8-row groups, 128
+// bytes between the two 16-byte K chunks). One stage of one slice is therefore one
+// contiguous 4 KiB (2 KiB) block that a single bulk copy moves into shared memory.
 //
-// Launches: slice pass (one warp per 32 operand rows) + product pass:
-//   tcgen05 kernel (default): one CTA per 128×64 output tile; one thread streams the
-//   S slice stages of A and B with cp.async.bulk into a two-stage shared-memory ring and
-//   issues tcgen05.mma.kind::i8 (M=128, N=64, K=32) into S int32 accumulators held in
-//   tensor memory (S·64 of 512 columns); four warps read the accumulators back with
-//   tcgen05.ld and recombine them in FP64.
+// Launches: exponent pass + slice pass (warp tasks of 32 rows × 64 K) + product pass:
+//   tcgen05 kernel (default): one CTA per 128×64 output tile (and K range, when the K loop
+//   is split across CTAs); one thread streams the S slice stages of A and B with
+//   cp.async.bulk into a four-stage shared-memory ring and issues tcgen05.mma.kind::i8
+//   (M=128, N=64, K=32) into S int32 accumulators held in tensor memory (S·64 of 512
+//   columns); four warps read the accumulators back with tcgen05.ld and recombine them in
+//   FP64.
 //   mma.sync kernel (TKB_SPLIT_KERNEL=mma): the same products with int8 mma.sync.
 #include <algorithm>
 #include <cmath>
@@ -40,7 +41,8 @@
 namespace {
 
 constexpr int PANEL_A = 128, PANEL_B = 64;   // rows per panel
-constexpr int KSTAGE = 64;                   // bytes of K per stage
+constexpr int KSTAGE = 32;                   // bytes of K per stage (one tensor-core K step)
+constexpr int NSTAGE = 4;                    // depth of the shared-memory ring
 constexpr int SMAX = 7;
 
 struct SliceJob {
@@ -55,8 +57,8 @@ struct CDbl {
 // byte offset of (row r, K byte kb) inside one slice plane
 __host__ __device__ __forceinline__ int64_t slice_off(int64_t r, int64_t kb, int64_t kpad, int pr) {
   const int64_t panel = r / pr, rr = r % pr;
-  const int64_t stg = kb >> 6, kk = kb & 63;
-  return panel * (pr * kpad) + stg * (pr * KSTAGE) + (rr >> 3) * 512 + (kk >> 4) * 128 +
+  const int64_t stg = kb >> 5, kk = kb & 31;
+  return panel * (pr * kpad) + stg * (pr * KSTAGE) + (rr >> 3) * 256 + (kk >> 4) * 128 +
          (rr & 7) * 16 + (kk & 15);
 }
 
@@ -91,122 +93,193 @@ __device__ __forceinline__ double op_elem(const GBlock &b, int operand, int cplx
   return (b.opB == TKB_OP_C) ? -im : im;
 }
 
-// One CTA (8 warps) per group of 32 operand rows (rows of all jobs enumerated through the
-// group prefix sums; padding rows included so padded slices are zero-filled).
-// Row-contiguous operands (real op(A) = A, real op(B) = Bᵀ) use lane = row: the K range is
-// cut into 16-element chunks dealt round-robin to the 8 warps, loads are coalesced across
-// lanes (16 independent loads per lane per chunk), the row maxima are combined through
-// shared memory, and each lane packs 16 K bytes per slice into one 16-byte store.
-// Other operands use lane = K position, four rows per warp.
+// Slicing of the operands, in two launches over fine-grained warp tasks. A task is one
+// group of 32 operand rows × one chunk of 128 K positions (rows of all jobs enumerated
+// through the task prefix sums; padding rows and padding K included, so the padded
+// slices are written as zeros).
+//   expo_kernel : per task the partial row maxima, folded into the row exponents with an
+//                 integer atomicMax (the exponent array starts at a very negative value,
+//                 byte 0x80 everywhere); complex row pairs fold into both rows.
+//   slice_kernel: per task the S slices of every element, packed into 16-byte (row-
+//                 contiguous operands, lane = row) or 4-byte (lane = 4 consecutive K)
+//                 stores in the tensor-core operand layout.
+// Row-contiguous operands are real op(A) = A and real op(B) = Bᵀ (consecutive rows are
+// consecutive addresses); the others read 4 consecutive K positions per lane.
+constexpr int KCHUNK = 64;
+
+struct TaskLoc {
+  SliceJob job;
+  int64_t r0, l0;
+};
+
+__device__ __forceinline__ TaskLoc locate_task(int64_t t, const int64_t *__restrict__ task_begin,
+                                               const SliceJob *__restrict__ jobs, int njobs,
+                                               const GBlock *__restrict__ blocks) {
+  int lo = 0, hi = njobs - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (task_begin[mid] <= t) lo = mid; else hi = mid - 1;
+  }
+  const SliceJob job = jobs[lo];
+  const GBlock &b = blocks[job.block];
+  const int64_t nkc = (b.kpad + KCHUNK - 1) / KCHUNK;
+  const int64_t rel = t - task_begin[lo];
+  return TaskLoc{job, (rel / nkc) * 32, (rel % nkc) * KCHUNK};
+}
+
+__device__ __forceinline__ bool row_contiguous(const GBlock &b, int op, int cplx) {
+  return !cplx && ((op == 0 && b.opA == TKB_OP_N) || (op == 1 && b.opB != TKB_OP_N));
+}
+
+__global__ void __launch_bounds__(256)
+    expo_kernel(const GBlock *__restrict__ blocks, const int64_t *__restrict__ task_begin,
+                const SliceJob *__restrict__ jobs, int njobs, int64_t ntasks, int cplx,
+                const double *__restrict__ A, const double *__restrict__ B, int8_t *ws) {
+  const int lane = threadIdx.x & 31;
+  const int64_t nw = (int64_t)gridDim.x * (blockDim.x >> 5);
+  for (int64_t t = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); t < ntasks; t += nw) {
+    const TaskLoc L = locate_task(t, task_begin, jobs, njobs, blocks);
+    const GBlock &b = blocks[L.job.block];
+    const int op = L.job.operand;
+    const int64_t Mlog = op == 0 ? (cplx ? 2 * b.m : b.m) : b.n;
+    const int64_t Klog = cplx ? 2 * b.k : b.k;
+    int32_t *expo = reinterpret_cast<int32_t *>(ws + (op == 0 ? b.wsEA : b.wsEB));
+    const double *X = op == 0 ? A : B;
+    const int64_t l1 = min(L.l0 + KCHUNK, Klog);
+    if (row_contiguous(b, op, cplx)) {
+      const int64_t xo = op == 0 ? b.offA : b.offB;
+      const int64_t ld = op == 0 ? b.lda : b.ldb;
+      const int64_t r = L.r0 + lane;
+      if (r >= Mlog || L.l0 >= l1) continue;
+      double mx = 0.0;
+      for (int64_t c = L.l0; c < l1; c += 16) {
+        double v[16];
+#pragma unroll
+        for (int q = 0; q < 16; ++q) v[q] = (c + q < l1) ? X[xo + r + (c + q) * ld] : 0.0;
+#pragma unroll
+        for (int q = 0; q < 16; ++q) mx = fmax(mx, fabs(v[q]));
+      }
+      if (mx > 0.0) {
+        int e;
+        frexp(mx, &e);
+        atomicMax(&expo[r], e);
+      }
+      continue;
+    }
+    // lane = 2 consecutive K positions; 8 rows per batch so 16 loads are in flight per lane
+    for (int rb = 0; rb < 32; rb += 8) {
+      double mx[8];
+#pragma unroll
+      for (int rr = 0; rr < 8; ++rr) {
+        const int64_t r = L.r0 + rb + rr;
+        mx[rr] = 0.0;
+#pragma unroll
+        for (int q = 0; q < 2; ++q) {
+          const int64_t l = L.l0 + 2 * lane + q;
+          if (r < Mlog && l < l1) mx[rr] = fmax(mx[rr], fabs(op_elem(b, op, cplx, X, r, l)));
+        }
+      }
+#pragma unroll
+      for (int rr = 0; rr < 8; ++rr) {
+        const int64_t r = L.r0 + rb + rr;
+        double m = mx[rr];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+        if (lane == 0 && r < Mlog && m > 0.0) {
+          int e;
+          frexp(m, &e);
+          atomicMax(&expo[r], e);
+          if (cplx && op == 0) atomicMax(&expo[r ^ 1], e);  // a complex row pair shares one exponent
+        }
+      }
+    }
+  }
+}
+
+template <int S>
+__device__ __forceinline__ void cut(double x, uint32_t (&w)[S], int shift) {
+#pragma unroll
+  for (int s = 0; s < S; ++s) {
+    x *= 128.0;
+    const double qd = trunc(x);
+    x -= qd;
+    w[s] |= ((uint32_t)(uint8_t)(int8_t)qd) << shift;
+  }
+}
+
 template <int S>
 __global__ void __launch_bounds__(256)
-    slice_kernel(const GBlock *__restrict__ blocks, const int64_t *__restrict__ grp_begin,
-                 const SliceJob *__restrict__ jobs, int njobs, int64_t ngroups, int cplx,
+    slice_kernel(const GBlock *__restrict__ blocks, const int64_t *__restrict__ task_begin,
+                 const SliceJob *__restrict__ jobs, int njobs, int64_t ntasks, int cplx,
                  const double *__restrict__ A, const double *__restrict__ B, int8_t *ws) {
-  __shared__ double red[8][32];
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  for (int64_t grp = blockIdx.x; grp < ngroups; grp += gridDim.x) {
-    int lo = 0, hi = njobs - 1;
-    while (lo < hi) {
-      const int mid = (lo + hi + 1) >> 1;
-      if (grp_begin[mid] <= grp) lo = mid; else hi = mid - 1;
-    }
-    const SliceJob job = jobs[lo];
-    const GBlock &b = blocks[job.block];
-    const int64_t r0 = (grp - grp_begin[lo]) * 32;
-    const int op = job.operand;
+  const int lane = threadIdx.x & 31;
+  const int64_t nw = (int64_t)gridDim.x * (blockDim.x >> 5);
+  for (int64_t t = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); t < ntasks; t += nw) {
+    const TaskLoc L = locate_task(t, task_begin, jobs, njobs, blocks);
+    const GBlock &b = blocks[L.job.block];
+    const int op = L.job.operand;
     const int64_t Mlog = op == 0 ? (cplx ? 2 * b.m : b.m) : b.n;
     const int64_t Klog = cplx ? 2 * b.k : b.k;
     const int64_t rows_pad = op == 0 ? b.mpad : b.npad;
     const int pr = op == 0 ? PANEL_A : PANEL_B;
     const int64_t kpad = b.kpad;
     int8_t *base = ws + (op == 0 ? b.wsA : b.wsB);
-    int32_t *expo = reinterpret_cast<int32_t *>(ws + (op == 0 ? b.wsEA : b.wsEB));
+    const int32_t *expo = reinterpret_cast<const int32_t *>(ws + (op == 0 ? b.wsEA : b.wsEB));
     const double *X = op == 0 ? A : B;
     const int64_t plane = rows_pad * kpad;
-    const bool row_contig = !cplx && ((op == 0 && b.opA == TKB_OP_N) || (op == 1 && b.opB != TKB_OP_N));
-    if (row_contig) {
-      // element (r, l) at X[xo + r + l * ld]
+    const int64_t l1 = min(L.l0 + KCHUNK, kpad);
+    if (row_contiguous(b, op, cplx)) {
       const int64_t xo = op == 0 ? b.offA : b.offB;
       const int64_t ld = op == 0 ? b.lda : b.ldb;
-      const int64_t r = r0 + lane;
+      const int64_t r = L.r0 + lane;
       const bool valid = r < Mlog;
-      const int64_t nchunk = (Klog + 15) / 16;
-      double mx = 0.0;
-      if (valid) {
-        for (int64_t c = warp; c < nchunk; c += 8) {
-          double v[16];
+      const int e = valid ? max(expo[r], -1100) : 0;
+      for (int64_t c = L.l0; c < l1; c += 16) {
+        uint32_t w[4][S];
 #pragma unroll
-          for (int q = 0; q < 16; ++q) {
-            const int64_t l = c * 16 + q;
-            v[q] = l < Klog ? X[xo + r + l * ld] : 0.0;
-          }
+        for (int h = 0; h < 4; ++h)
 #pragma unroll
-          for (int q = 0; q < 16; ++q) mx = fmax(mx, fabs(v[q]));
-        }
-      }
-      red[warp][lane] = mx;
-      __syncthreads();
-      mx = 0.0;
-#pragma unroll
-      for (int w = 0; w < 8; ++w) mx = fmax(mx, red[w][lane]);
-      __syncthreads();
-      int e = 0;
-      if (mx > 0.0) frexp(mx, &e);  // mx < 2^e
-      if (warp == 0) expo[r] = e;
-      for (int64_t c = warp; c < kpad / 16; c += 8) {
-        const int64_t l0 = c * 16;
+          for (int s = 0; s < S; ++s) w[h][s] = 0u;
         double v[16];
 #pragma unroll
-        for (int q = 0; q < 16; ++q) {
-          const int64_t l = l0 + q;
-          v[q] = (valid && l < Klog) ? X[xo + r + l * ld] : 0.0;
-        }
-        uint32_t w[S][4];
+        for (int q = 0; q < 16; ++q) v[q] = (valid && c + q < Klog) ? X[xo + r + (c + q) * ld] : 0.0;
 #pragma unroll
-        for (int s = 0; s < S; ++s) w[s][0] = w[s][1] = w[s][2] = w[s][3] = 0u;
-#pragma unroll
-        for (int q = 0; q < 16; ++q) {
-          double x = ldexp(v[q], -e);
-#pragma unroll
-          for (int s = 0; s < S; ++s) {
-            x *= 128.0;
-            const double qd = trunc(x);
-            x -= qd;
-            w[s][q >> 2] |= ((uint32_t)(uint8_t)(int8_t)qd) << (8 * (q & 3));
-          }
-        }
-        const int64_t off = slice_off(r, l0, kpad, pr);
+        for (int q = 0; q < 16; ++q) cut<S>(ldexp(v[q], -e), w[q >> 2], 8 * (q & 3));
+        const int64_t off = slice_off(r, c, kpad, pr);
 #pragma unroll
         for (int s = 0; s < S; ++s)
-          *reinterpret_cast<uint4 *>(base + s * plane + off) = make_uint4(w[s][0], w[s][1], w[s][2], w[s][3]);
+          *reinterpret_cast<uint4 *>(base + s * plane + off) = make_uint4(w[0][s], w[1][s], w[2][s], w[3][s]);
       }
       continue;
     }
-    for (int rr = warp * 4; rr < warp * 4 + 4; ++rr) {
-      const int64_t r = r0 + rr;
-      const bool valid = r < Mlog;
-      double mx = 0.0;
-      if (valid) {
-        for (int64_t l = lane; l < Klog; l += 32) mx = fmax(mx, fabs(op_elem(b, op, cplx, X, r, l)));
-        if (cplx && op == 0)  // a complex row pair shares one exponent
-          for (int64_t l = lane; l < Klog; l += 32) mx = fmax(mx, fabs(op_elem(b, op, cplx, X, r ^ 1, l)));
-      }
+    // lane = 2 consecutive K positions (64 per warp); 8 rows per batch, loads first
+    const int64_t lb = L.l0 + 2 * lane;
+    for (int rb = 0; rb < 32; rb += 8) {
+      double v[8][2];
+      int ex[8];
 #pragma unroll
-      for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
-      int e = 0;
-      if (mx > 0.0) frexp(mx, &e);
-      if (lane == 0) expo[r] = e;
-      for (int64_t l = lane; l < kpad; l += 32) {
-        double x = (valid && l < Klog) ? ldexp(op_elem(b, op, cplx, X, r, l), -e) : 0.0;
-        const int64_t off = slice_off(r, l, kpad, pr);
+      for (int rr = 0; rr < 8; ++rr) {
+        const int64_t r = L.r0 + rb + rr;
+        const bool valid = r < Mlog;
+        ex[rr] = valid ? max(expo[r], -1100) : 0;
 #pragma unroll
-        for (int s = 0; s < S; ++s) {
-          x *= 128.0;
-          const double qd = trunc(x);
-          x -= qd;
-          base[s * plane + off] = (int8_t)qd;
+        for (int q = 0; q < 2; ++q) {
+          const int64_t l = lb + q;
+          v[rr][q] = (valid && l < Klog) ? op_elem(b, op, cplx, X, r, l) : 0.0;
         }
+      }
+      if (lb >= l1) continue;
+#pragma unroll
+      for (int rr = 0; rr < 8; ++rr) {
+        const int64_t r = L.r0 + rb + rr;
+        uint32_t w[S];
+#pragma unroll
+        for (int s = 0; s < S; ++s) w[s] = 0u;
+#pragma unroll
+        for (int q = 0; q < 2; ++q) cut<S>(ldexp(v[rr][q], -ex[rr]), w, 8 * q);
+        const int64_t off = slice_off(r, lb, kpad, pr);
+#pragma unroll
+        for (int s = 0; s < S; ++s) *reinterpret_cast<uint16_t *>(base + s * plane + off) = (uint16_t)w[s];
       }
     }
   }
@@ -319,30 +392,44 @@ constexpr uint32_t kTmemCols = 512;
 // both K-major, N = 64 (bits 17-22 = 64>>3), M = 128 (bits 24-28 = 128>>4)
 constexpr uint32_t kIdescI8 = (2u << 4) | (1u << 7) | (1u << 10) | ((64u >> 3) << 17) | ((128u >> 4) << 24);
 
+// One product task: output tile (m0, n0) of a block, K stages [kb, ke). When a tile's K
+// range is split over nsplit CTAs (few tiles, long K), each CTA recombines its own int32
+// diagonals into an FP64 partial tile and stores it (plain coalesced stores) in partial
+// buffer pbase + sid; the CTA that arrives last on the tile's counter adds the partials in
+// split order (deterministic), scales, writes C and resets the counter for the next launch.
+struct SplitTile {
+  int32_t block, m0, n0, kind;
+  int32_t kb, ke, slot, nsplit;
+  int32_t sid, pbase;
+};
+
 template <int S>
 __global__ void __launch_bounds__(128, 1)
-    gemm_split_tc_kernel(const GBlock *__restrict__ blocks, const GTile *__restrict__ tiles,
+    gemm_split_tc_kernel(const GBlock *__restrict__ blocks, const SplitTile *__restrict__ tiles,
                          const int8_t *__restrict__ ws, int cplx, double *__restrict__ C, CDbl alpha,
-                         CDbl beta, int *err) {
+                         CDbl beta, int *err, double *__restrict__ part, int *__restrict__ pcnt) {
   constexpr uint32_t A_BYTES = S * PANEL_A * KSTAGE, B_BYTES = S * PANEL_B * KSTAGE;
   constexpr uint32_t STAGE = A_BYTES + B_BYTES;
   extern __shared__ __align__(1024) unsigned char smem[];
-  uint64_t *full = reinterpret_cast<uint64_t *>(smem + 2 * STAGE);
-  uint64_t *empty = full + 2;
-  uint64_t *done = full + 4;
-  uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(full + 6);
+  uint64_t *full = reinterpret_cast<uint64_t *>(smem + NSTAGE * STAGE);
+  uint64_t *empty = full + NSTAGE;
+  uint64_t *done = full + 2 * NSTAGE;
+  uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(full + 2 * NSTAGE + 1);
+  int *ticket = reinterpret_cast<int *>(full + 2 * NSTAGE + 2);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const GTile tile = tiles[blockIdx.x];
+  const SplitTile tile = tiles[blockIdx.x];
   const GBlock b = blocks[tile.block];
   const bool has_k = tile.kind == 0;
-  const int nk = has_k ? b.kpad / KSTAGE : 0;
+  const int kb = tile.kb;
+  const int nk = has_k ? tile.ke - tile.kb : 0;
   const bool bz = beta.x == 0.0 && beta.y == 0.0;
 
   if (tid == 0) {
-    mbar_init(&full[0], 1);
-    mbar_init(&full[1], 1);
-    mbar_init(&empty[0], 1);
-    mbar_init(&empty[1], 1);
+#pragma unroll
+    for (int st = 0; st < NSTAGE; ++st) {
+      mbar_init(&full[st], 1);
+      mbar_init(&empty[st], 1);
+    }
     mbar_init(done, 1);
     asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
   }
@@ -360,56 +447,63 @@ __global__ void __launch_bounds__(128, 1)
     const int8_t *gA = ws + b.wsA + (int64_t)(tile.m0 / PANEL_A) * PANEL_A * b.kpad;
     const int8_t *gB = ws + b.wsB + (int64_t)(tile.n0 / PANEL_B) * PANEL_B * b.kpad;
     const int64_t planeA = (int64_t)b.mpad * b.kpad, planeB = (int64_t)b.npad * b.kpad;
-    auto load = [&](int kt, int st) {
+    auto load = [&](int kt, int st) {  // kt: local stage index, global stage kb + kt
       unsigned char *sa = smem + st * STAGE;
+      const int64_t kg = kb + kt;
       mbar_expect_tx(&full[st], STAGE);
 #pragma unroll
       for (int s = 0; s < S; ++s)
-        bulk_g2s(sa + s * (PANEL_A * KSTAGE), gA + s * planeA + (int64_t)kt * PANEL_A * KSTAGE,
+        bulk_g2s(sa + s * (PANEL_A * KSTAGE), gA + s * planeA + kg * PANEL_A * KSTAGE,
                  PANEL_A * KSTAGE, &full[st]);
 #pragma unroll
       for (int s = 0; s < S; ++s)
-        bulk_g2s(sa + A_BYTES + s * (PANEL_B * KSTAGE), gB + s * planeB + (int64_t)kt * PANEL_B * KSTAGE,
+        bulk_g2s(sa + A_BYTES + s * (PANEL_B * KSTAGE), gB + s * planeB + kg * PANEL_B * KSTAGE,
                  PANEL_B * KSTAGE, &full[st]);
     };
+    // NSTAGE-deep ring: stage kt lives in slot kt % NSTAGE; its n-th use has parity n & 1.
+    // After issuing the products of stage kt, the slot of stage kt-1 is refilled with stage
+    // kt-1+NSTAGE once those older products have drained (their commit on empty[]), so the
+    // tensor pipe always has the current stage queued while the copy engine refills.
     bool ok = true;
     int issued = 0, consumed = 0;  // stages loaded / waited on
-    load(0, 0);
-    issued = 1;
+    for (; issued < nk && issued < NSTAGE; ++issued) load(issued, issued);
+    // descriptor templates: only the start address changes between stages
+    const uint32_t ring0 = smem_u32(smem);
     for (int kt = 0; kt < nk && ok; ++kt) {
-      const int st = kt & 1;
-      if (kt + 1 < nk) {
-        const int st2 = (kt + 1) & 1;
-        if (kt + 1 >= 2) ok = mbar_wait(&empty[st2], ((kt + 1) / 2 - 1) & 1);
-        if (!ok) break;
-        load(kt + 1, st2);
-        ++issued;
-      }
-      ok = mbar_wait(&full[st], (kt / 2) & 1);
+      const int st = kt % NSTAGE;
+      ok = mbar_wait(&full[st], (kt / NSTAGE) & 1);
       if (!ok) break;
       ++consumed;
       tc_fence_after();
-      const uint32_t a0 = smem_u32(smem + st * STAGE), b0 = a0 + A_BYTES;
+      const uint32_t a0 = ring0 + st * STAGE, b0 = a0 + A_BYTES;
+      uint64_t ad[S], bd[S];
 #pragma unroll
-      for (int j = 0; j < KSTAGE / 32; ++j) {
+      for (int s = 0; s < S; ++s) {
+        ad[s] = umma_desc(a0 + s * (PANEL_A * KSTAGE), 128, 256);
+        bd[s] = umma_desc(b0 + s * (PANEL_B * KSTAGE), 128, 256);
+      }
 #pragma unroll
-        for (int s = 0; s < S; ++s) {
-          const uint64_t ad = umma_desc(a0 + s * (PANEL_A * KSTAGE) + j * 256, 128, 512);
+      for (int s = 0; s < S; ++s) {
 #pragma unroll
-          for (int t = 0; t < S - s; ++t) {
-            const uint64_t bd = umma_desc(b0 + t * (PANEL_B * KSTAGE) + j * 256, 128, 512);
-            const uint32_t acc = (kt > 0 || j > 0 || s > 0) ? 1u : 0u;
-            umma_i8(tmem + (uint32_t)((s + t) * 64), ad, bd, kIdescI8, acc);
-          }
-        }
+        for (int t = 0; t < S - s; ++t)
+          umma_i8(tmem + (uint32_t)((s + t) * 64), ad[s], bd[t], kIdescI8, (kt > 0 || s > 0) ? 1u : 0u);
       }
       umma_commit(&empty[st]);
+      if (kt >= 1) {
+        const int prev = kt - 1, ps = prev % NSTAGE, nxt = prev + NSTAGE;
+        if (nxt < nk) {
+          ok = mbar_wait(&empty[ps], (prev / NSTAGE) & 1);
+          if (!ok) break;
+          load(nxt, ps);
+          ++issued;
+        }
+      }
     }
     umma_commit(done);
     if (!ok) {
       atomicExch(err, 1);
       // let every bulk copy still in flight land before the CTA can exit (bounded)
-      for (int k = consumed; k < issued; ++k) mbar_wait(&full[k & 1], (k / 2) & 1);
+      for (int k = consumed; k < issued; ++k) mbar_wait(&full[k % NSTAGE], (k / NSTAGE) & 1);
     }
   }
   if (has_k) {
@@ -421,29 +515,64 @@ __global__ void __launch_bounds__(128, 1)
   const int32_t *eA = reinterpret_cast<const int32_t *>(ws + b.wsEA);
   const int32_t *eB = reinterpret_cast<const int32_t *>(ws + b.wsEB);
   const int64_t Mreal = cplx ? 2 * b.m : b.m;
-  const int64_t i = tile.m0 + 32 * warp + lane;
-  const int ei = (has_k && i < Mreal) ? eA[i] : 0;
-#pragma unroll 1
-  for (int c = 0; c < 4; ++c) {
-    double v[16];
+  const int row = 32 * warp + lane;
+  const int64_t i = tile.m0 + row;
+  // exponents of all-zero rows stay at the 0x80808080 reset value: clamp before adding
+  const int ei = (has_k && i < Mreal) ? max(eA[i], -1100) : 0;
+  // this CTA's FP64 recombination of its diagonals: chunk c of 16 columns
+  auto recombine = [&](int c, double (&v)[16]) {
 #pragma unroll
     for (int q = 0; q < 16; ++q) v[q] = 0.0;
-    if (has_k) {
+    if (!has_k) return;
 #pragma unroll
-      for (int d = S - 1; d >= 0; --d) {
-        uint32_t r[16];
-        tmem_ld16(tmem + ((uint32_t)(32 * warp) << 16) + (uint32_t)(d * 64 + c * 16), r);
+    for (int d = S - 1; d >= 0; --d) {
+      uint32_t r[16];
+      tmem_ld16(tmem + ((uint32_t)(32 * warp) << 16) + (uint32_t)(d * 64 + c * 16), r);
 #pragma unroll
-        for (int q = 0; q < 16; ++q) v[q] += ldexp((double)(int32_t)r[q], -7 * (d + 2));
+      for (int q = 0; q < 16; ++q) v[q] += ldexp((double)(int32_t)r[q], -7 * (d + 2));
+    }
+  };
+  bool write_out = true;
+  if (tile.nsplit > 1) {
+    double *mine = part + (int64_t)(tile.pbase + tile.sid) * (64 * 128);  // [col][row]
+#pragma unroll 1
+    for (int c = 0; c < 4; ++c) {
+      double v[16];
+      recombine(c, v);
+#pragma unroll
+      for (int q = 0; q < 16; ++q) __stcg(&mine[(c * 16 + q) * 128 + row], v[q]);
+    }
+    __threadfence();
+    __syncthreads();
+    if (tid == 0) *ticket = atomicAdd(&pcnt[tile.slot], 1);
+    __syncthreads();
+    write_out = (*ticket == tile.nsplit - 1);
+    if (write_out) __threadfence();
+  }
+  if (write_out) {
+#pragma unroll 1
+    for (int c = 0; c < 4; ++c) {
+      double v[16];
+      if (tile.nsplit > 1) {
+#pragma unroll
+        for (int q = 0; q < 16; ++q) v[q] = 0.0;
+        for (int sp = 0; sp < tile.nsplit; ++sp) {
+          const double *src = part + (int64_t)(tile.pbase + sp) * (64 * 128);
+#pragma unroll
+          for (int q = 0; q < 16; ++q) v[q] += __ldcg(&src[(c * 16 + q) * 128 + row]);
+        }
+      } else {
+        recombine(c, v);
+      }
+#pragma unroll
+      for (int q = 0; q < 16; ++q) {
+        const int64_t j = tile.n0 + c * 16 + q;
+        double val = v[q];
+        if (has_k) val = ldexp(val, ei + ((j < b.n) ? max(eB[j], -1100) : 0));
+        store_out(val, i, j, b, cplx, C, alpha, beta, bz, 1);
       }
     }
-#pragma unroll
-    for (int q = 0; q < 16; ++q) {
-      const int64_t j = tile.n0 + c * 16 + q;
-      double val = v[q];
-      if (has_k) val = ldexp(val, ei + ((j < b.n) ? eB[j] : 0));
-      store_out(val, i, j, b, cplx, C, alpha, beta, bz, 1);
-    }
+    if (tile.nsplit > 1 && tid == 0) pcnt[tile.slot] = 0;
   }
   tc_fence_before();
   __syncthreads();
@@ -587,7 +716,7 @@ __global__ void __launch_bounds__(256)
               if (tile.kind == 0) {
 #pragma unroll
                 for (int d = S - 1; d >= 0; --d) v += ldexp((double)acc[d][mt][nt][hr * 2 + hc], -7 * (d + 2));
-                v = ldexp(v, ((i < Mreal) ? eA[i] : 0) + ((j < b.n) ? eB[j] : 0));
+                v = ldexp(v, ((i < Mreal) ? max(eA[i], -1100) : 0) + ((j < b.n) ? max(eB[j], -1100) : 0));
               }
               store_out(v, i, j, b, cplx, C, alpha, beta, bz, 4);
             }
@@ -614,12 +743,17 @@ template <int S>
 int launch_split(tkb_ctx *ctx, const tkb_plan *p, void *C, const void *A, const void *B, CDbl a, CDbl b) {
   const int cplx = p->dtype == TKB_C128 ? 1 : 0;
   if (p->nsrows > 0) {
-    // one CTA per 32-row group
-    const int grid = (int)std::min<int64_t>(p->nsrows, (int64_t)ctx->num_sms * 8);
+    // one warp per (32-row group, 128-K chunk) task
+    const int grid = (int)std::min<int64_t>((p->nsrows + 7) / 8, (int64_t)ctx->num_sms * 16);
+    int8_t *ws = (int8_t *)ctx->ws;
+    TKB_CUDA_TRY(ctx, cudaMemsetAsync(ws + p->expo_off, 0x80, p->expo_bytes, ctx->stream));
+    expo_kernel<<<grid, 256, 0, ctx->stream>>>(p->blocks, p->srow_begin, (const SliceJob *)p->sjobs,
+                                               p->nsjobs, p->nsrows, cplx, (const double *)A,
+                                               (const double *)B, ws);
     slice_kernel<S><<<grid, 256, 0, ctx->stream>>>(p->blocks, p->srow_begin, (const SliceJob *)p->sjobs,
                                                    p->nsjobs, p->nsrows, cplx, (const double *)A,
-                                                   (const double *)B, (int8_t *)ctx->ws);
-    ctx->launches++;
+                                                   (const double *)B, ws);
+    ctx->launches += 2;
     TKB_CUDA_TRY(ctx, cudaGetLastError());
   }
   if (use_mma_sync()) {
@@ -630,11 +764,12 @@ int launch_split(tkb_ctx *ctx, const tkb_plan *p, void *C, const void *A, const 
     k<<<grid, 256, smem, ctx->stream>>>(p->blocks, p->stiles, (int)p->nstiles, ctx->counters,
                                         (const int8_t *)ctx->ws, cplx, (double *)C, a, b);
   } else {
-    const size_t smem = 2 * (size_t)S * (PANEL_A + PANEL_B) * KSTAGE + 64;
+    const size_t smem = NSTAGE * (size_t)S * (PANEL_A + PANEL_B) * KSTAGE + 128;
     auto k = gemm_split_tc_kernel<S>;
     TKB_CUDA_TRY(ctx, cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    k<<<(int)p->nstiles, 128, smem, ctx->stream>>>(p->blocks, p->stiles, (const int8_t *)ctx->ws, cplx,
-                                                   (double *)C, a, b, ctx->counters + 8);
+    k<<<(int)p->nkstiles, 128, smem, ctx->stream>>>(p->blocks, (const SplitTile *)p->kstiles,
+                                                    (const int8_t *)ctx->ws, cplx, (double *)C, a, b,
+                                                    ctx->counters + 8, p->part, p->pcnt);
   }
   ctx->launches++;
   TKB_CUDA_TRY(ctx, cudaGetLastError());
@@ -669,34 +804,79 @@ int tkb_gemm_split_prepare(tkb_ctx *ctx, tkb_plan *p) {
     b.wsB = (int64_t)off;
     off += (size_t)S * b.npad * b.kpad;
     off = roundup((int64_t)off, 256);
-    b.wsEA = (int64_t)off;
-    off += (size_t)b.mpad * 4;
-    b.wsEB = (int64_t)off;
-    off += (size_t)b.npad * 4;
-    off = roundup((int64_t)off, 256);
     const int kind = b.k > 0 ? 0 : 1;
     if (kind == 0) {
+      const int64_t nkc = (b.kpad + KCHUNK - 1) / KCHUNK;  // K chunks (slicing tasks per row group)
       jobs.push_back({(int32_t)bi, 0});
       grp_begin.push_back(ngroups);
-      ngroups += b.mpad / 32;
+      ngroups += (b.mpad / 32) * nkc;
       jobs.push_back({(int32_t)bi, 1});
       grp_begin.push_back(ngroups);
-      ngroups += b.npad / 32;
+      ngroups += (b.npad / 32) * nkc;
     }
     for (int64_t m0 = 0; m0 < M; m0 += PANEL_A)
       for (int64_t n0 = 0; n0 < b.n; n0 += PANEL_B) tiles.push_back({(int32_t)bi, (int32_t)m0, (int32_t)n0, kind});
   }
+  // exponent arrays of every block in one contiguous region (reset to byte 0x80 per launch)
+  p->expo_off = (int64_t)off;
+  for (size_t bi = 0; bi < p->hblocks.size(); ++bi) {
+    GBlock &b = p->hblocks[bi];
+    if (b.m == 0 || b.n == 0 || b.skinny) continue;
+    b.wsEA = (int64_t)off;
+    off += (size_t)b.mpad * 4;
+    b.wsEB = (int64_t)off;
+    off += (size_t)b.npad * 4;
+  }
+  p->expo_bytes = (int64_t)off - p->expo_off;
+  off = roundup((int64_t)off, 256);
   std::stable_sort(tiles.begin(), tiles.end(), [&](const GTile &x, const GTile &y) {
     return p->hblocks[x.block].kpad > p->hblocks[y.block].kpad;
   });
+  // tcgen05 tasks: split the K range of tiles when there are too few tiles to occupy every
+  // SM twice, keeping at least two K stages per task
+  std::vector<SplitTile> kt;
+  int nslots = 0, npart = 0;
+  {
+    const int64_t nt = (int64_t)tiles.size();
+    int KS = 1;
+    // one CTA per SM (shared-memory ring): keep every task in the first wave
+    if (nt > 0 && nt < (int64_t)ctx->num_sms)
+      KS = (int)std::min<int64_t>(8, (int64_t)ctx->num_sms / nt);
+    for (const GTile &t : tiles) {
+      const int nk = p->hblocks[t.block].kpad / KSTAGE;
+      const int ks = t.kind == 0 ? std::max(1, std::min(KS, nk / 4)) : 1;  // ≥ 4 K stages per task
+      if (ks == 1) {
+        kt.push_back({t.block, t.m0, t.n0, t.kind, 0, nk, -1, 1, 0, 0});
+      } else {
+        const int slot = nslots++;
+        for (int s = 0; s < ks; ++s)
+          kt.push_back({t.block, t.m0, t.n0, t.kind, s * nk / ks, (s + 1) * nk / ks, slot, ks, s, npart});
+        npart += ks;
+      }
+    }
+    std::stable_sort(kt.begin(), kt.end(), [](const SplitTile &x, const SplitTile &y) {
+      return (x.ke - x.kb) > (y.ke - y.kb);
+    });
+  }
   p->ws_bytes = off;
   p->nstiles = (int64_t)tiles.size();
+  p->nkstiles = (int64_t)kt.size();
   p->nsjobs = (int)jobs.size();
   p->nsrows = ngroups;
   cudaError_t e = cudaSuccess;
   if (!tiles.empty()) {
     e = cudaMalloc((void **)&p->stiles, tiles.size() * sizeof(GTile));
     if (e == cudaSuccess) e = cudaMemcpy(p->stiles, tiles.data(), tiles.size() * sizeof(GTile), cudaMemcpyHostToDevice);
+  }
+  if (e == cudaSuccess && !kt.empty()) {
+    e = cudaMalloc(&p->kstiles, kt.size() * sizeof(SplitTile));
+    if (e == cudaSuccess) e = cudaMemcpy(p->kstiles, kt.data(), kt.size() * sizeof(SplitTile), cudaMemcpyHostToDevice);
+  }
+  if (e == cudaSuccess && nslots > 0) {
+    const size_t pb = (size_t)npart * 64 * 128 * sizeof(double);
+    e = cudaMalloc((void **)&p->part, pb);
+    if (e == cudaSuccess) e = cudaMalloc((void **)&p->pcnt, nslots * sizeof(int));
+    if (e == cudaSuccess) e = cudaMemset(p->pcnt, 0, nslots * sizeof(int));
   }
   if (e == cudaSuccess && !jobs.empty()) {
     e = cudaMalloc(&p->sjobs, jobs.size() * sizeof(SliceJob));

@@ -64,7 +64,7 @@ struct tkb_table {
   TGroup *groups = nullptr;
   int64_t *sstr = nullptr, *soff = nullptr, *dstr = nullptr, *doff = nullptr;
   double *coeffs = nullptr;
-  int64_t *task_begin = nullptr;  // ngroups, for the device-side group lookup
+  int32_t *task_group = nullptr;  // ntasks: the group of every task
 };
 
 int tkb_transform_launch(tkb_ctx *ctx, const tkb_table *t, int dtype, void *dst,
@@ -110,6 +110,11 @@ struct tkb_plan {
   int64_t slice_rows_A = 0, slice_rows_B = 0;  // total padded rows for the slicing pass
   GTile *stiles = nullptr;      // tiles of the split kernel (different tile shape)
   int64_t nstiles = 0;
+  int64_t expo_off = 0, expo_bytes = 0;  // exponent region inside the workspace
+  void *kstiles = nullptr;      // tcgen05 product tasks (tile, K range, split slot)
+  int64_t nkstiles = 0;
+  double *part = nullptr;       // split-K FP64 partial tiles (rewritten every launch)
+  int *pcnt = nullptr;          // split-K arrival counters (self-clearing)
   void *sjobs = nullptr;        // slice jobs (block, operand)
   int64_t *srow_begin = nullptr;
   int nsjobs = 0;

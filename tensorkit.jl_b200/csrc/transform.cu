@@ -72,7 +72,7 @@ __device__ __forceinline__ double2 scalar_from<double2>(CDbl s) { return make_do
 
 template <typename T, bool CONJ>
 __global__ void __launch_bounds__(kThreads)
-    treetransform_kernel(const TGroup *__restrict__ groups, const int64_t *__restrict__ task_begin,
+    treetransform_kernel(const TGroup *__restrict__ groups, const int32_t *__restrict__ task_group,
                          int ngroups, int64_t ntasks, const int64_t *__restrict__ sstr,
                          const int64_t *__restrict__ soff, const int64_t *__restrict__ dstr,
                          const int64_t *__restrict__ doff, const double *__restrict__ coeffs,
@@ -84,14 +84,13 @@ __global__ void __launch_bounds__(kThreads)
   const T beta = scalar_from<T>(beta_);
   const bool bz = beta_zero != 0;
 
-  for (int64_t task = blockIdx.x; task < ntasks; task += gridDim.x) {
-    // locate the group: last g with task_begin[g] <= task
-    int lo = 0, hi = ngroups - 1;
-    while (lo < hi) {
-      int mid = (lo + hi + 1) >> 1;
-      if (task_begin[mid] <= task) lo = mid; else hi = mid - 1;
-    }
-    const TGroup &G = groups[lo];
+  // Each CTA walks a contiguous range of tasks (tasks of one group are contiguous, so the
+  // group metadata stays in L1); the task → group map was built on the host.
+  const int64_t per = (ntasks + gridDim.x - 1) / gridDim.x;
+  const int64_t t_begin = (int64_t)blockIdx.x * per;
+  const int64_t t_end = min(ntasks, t_begin + per);
+  for (int64_t task = t_begin; task < t_end; ++task) {
+    const TGroup &G = groups[task_group[task]];
     int64_t t = task - G.task_begin;
     const int64_t itb = t % G.ntile_b;
     t /= G.ntile_b;
@@ -250,7 +249,8 @@ extern "C" int tkb_table_create(tkb_ctx *ctx, const tkb_table_desc *d, tkb_table
 
   std::vector<TGroup> hg;
   hg.reserve(G);
-  std::vector<int64_t> hsstr, hsoff, hdstr, hdoff, htask;
+  std::vector<int64_t> hsstr, hsoff, hdstr, hdoff;
+  std::vector<int32_t> htask;  // task → group
   std::vector<double> hcoef;
   int64_t ntasks = 0, er = 0, ew = 0;
   size_t smem_max_f64 = 0, smem_max_c128 = 0;
@@ -422,7 +422,7 @@ extern "C" int tkb_table_create(tkb_ctx *ctx, const tkb_table_desc *d, tkb_table
       smem_max_c128 = std::max(smem_max_c128, (size_t)(nsrc * te) * el128);
     }
     max_trees = std::max<int>(max_trees, (int)nsrc);
-    htask.push_back(tg.task_begin);
+    htask.insert(htask.end(), (size_t)(ntasks - tg.task_begin), (int32_t)g);
     hg.push_back(tg);
   }
   if (std::max(smem_max_f64, smem_max_c128) > ctx->smem_optin)
@@ -447,7 +447,7 @@ extern "C" int tkb_table_create(tkb_ctx *ctx, const tkb_table_desc *d, tkb_table
   };
   cudaError_t e = cudaSetDevice(ctx->device);
   if (e == cudaSuccess) e = up((void **)&t->groups, hg.data(), hg.size() * sizeof(TGroup));
-  if (e == cudaSuccess) e = up((void **)&t->task_begin, htask.data(), htask.size() * 8);
+  if (e == cudaSuccess) e = up((void **)&t->task_group, htask.data(), htask.size() * 4);
   if (e == cudaSuccess) e = up((void **)&t->sstr, hsstr.data(), hsstr.size() * 8);
   if (e == cudaSuccess) e = up((void **)&t->soff, hsoff.data(), hsoff.size() * 8);
   if (e == cudaSuccess) e = up((void **)&t->dstr, hdstr.data(), hdstr.size() * 8);
@@ -465,7 +465,7 @@ extern "C" int tkb_table_create(tkb_ctx *ctx, const tkb_table_desc *d, tkb_table
 extern "C" int tkb_table_destroy(tkb_table *t) {
   if (!t) return TKB_OK;
   cudaFree(t->groups);
-  cudaFree(t->task_begin);
+  cudaFree(t->task_group);
   cudaFree(t->sstr);
   cudaFree(t->soff);
   cudaFree(t->dstr);
@@ -495,14 +495,14 @@ int tkb_transform_launch(tkb_ctx *ctx, const tkb_table *t, int dtype, void *dst,
     const size_t smem = t->smem_f64;
     auto k = treetransform_kernel<double, false>;
     if (smem > 48 * 1024) TKB_CUDA_TRY(ctx, cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    k<<<grid, kThreads, smem, ctx->stream>>>(t->groups, t->task_begin, t->ngroups, t->ntasks,
+    k<<<grid, kThreads, smem, ctx->stream>>>(t->groups, t->task_group, t->ngroups, t->ntasks,
                                             t->sstr, t->soff, t->dstr, t->doff, t->coeffs,
                                             (double *)dst, (const double *)src, a, b, bz);
   } else if (dtype == TKB_C128) {
     const size_t smem = t->smem_c128;
     auto k = conj ? treetransform_kernel<double2, true> : treetransform_kernel<double2, false>;
     if (smem > 48 * 1024) TKB_CUDA_TRY(ctx, cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    k<<<grid, kThreads, smem, ctx->stream>>>(t->groups, t->task_begin, t->ngroups, t->ntasks,
+    k<<<grid, kThreads, smem, ctx->stream>>>(t->groups, t->task_group, t->ngroups, t->ntasks,
                                             t->sstr, t->soff, t->dstr, t->doff, t->coeffs,
                                             (double2 *)dst, (const double2 *)src, a, b, bz);
   } else {
