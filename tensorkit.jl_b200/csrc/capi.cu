@@ -173,7 +173,8 @@ int tkb_gemm_plan_create(tkb_ctx *ctx, const tkb_gemm_desc *d, tkb_plan **out) {
       if (b.opB == TKB_OP_C) b.opB = TKB_OP_T;
     }
     flops += (d->dtype == TKB_C128 ? 8.0 : 2.0) * (double)b.m * (double)b.n * (double)b.k;
-    b.skinny = (b.n <= kSkinnyMax && b.k <= kSkinnyMax) ? 1 : 0;
+    b.skinny = (b.n <= kSkinnyMax && b.k <= kSkinnyMax && b.m >= kSkinnyMinRows) ? 1 : 0;
+    if (b.skinny && b.m > 0 && b.n > 0) p->sk_dim = std::max<int>(p->sk_dim, (int)std::max(b.n, b.k));
     p->hblocks.push_back(b);
     if (b.m > 0 && b.n > 0) {
       if (b.skinny) {

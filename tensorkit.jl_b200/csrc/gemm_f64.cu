@@ -371,47 +371,61 @@ __device__ __forceinline__ double2 scl(double2 v, CDbl a) {
   return make_double2(a.x * v.x - a.y * v.y, a.x * v.y + a.y * v.x);
 }
 
-template <typename T>
+// D bounds n and k of every block of the launch (4, 8 or 16): the row loops are unrolled to D,
+// so the code stays small for the common narrow bonds.
+template <typename T, bool BZ, int D>
 __global__ void __launch_bounds__(kSkinnyRows)
     gemm_skinny_kernel(const GBlock *__restrict__ blocks, const GTile *__restrict__ tasks, int64_t ntasks,
                        T *__restrict__ C, const T *__restrict__ A, const T *__restrict__ B, CDbl alpha,
                        CDbl beta) {
-  __shared__ T Bs[kSkinnyMax * kSkinnyMax];
-  const bool bz = beta.x == 0.0 && beta.y == 0.0;
+  __shared__ T Bs[D * D];
   for (int64_t ti = blockIdx.x; ti < ntasks; ti += gridDim.x) {
     const GTile tk = tasks[ti];
     const GBlock b = blocks[tk.block];
     const int n = (int)b.n, k = (int)b.k;
     __syncthreads();
-    for (int e = threadIdx.x; e < k * n; e += blockDim.x) {
-      const int l = e % k, j = e / k;  // op(B)(l, j)
+    // op(B)(l, j), zero outside k × n (the row loop below runs over the full D × D)
+    for (int e = threadIdx.x; e < D * D; e += blockDim.x) {
+      const int l = e % D, j = e / D;
       const int64_t idx = (b.opB == TKB_OP_N) ? b.offB + l + (int64_t)j * b.ldb : b.offB + j + (int64_t)l * b.ldb;
-      Bs[l + j * kSkinnyMax] = ldA<T>(B + idx, b.opB == TKB_OP_C);
+      Bs[e] = (l < k && j < n && tk.kind == 0) ? ldA<T>(B + idx, b.opB == TKB_OP_C) : zero(T{});
     }
     __syncthreads();
     const int64_t i = tk.m0 + threadIdx.x;
     if (i >= b.m) continue;
-    T acc[kSkinnyMax];
+    // the whole row of op(A) (and of C when β ≠ 0) is fetched before any arithmetic
+    // (k, n ≤ D), so the loads of a thread are all in flight together
+    const int kk = tk.kind == 0 ? k : 0;
+    const bool conjA = b.opA == TKB_OP_C;
+    const int64_t sa_l = (b.opA == TKB_OP_N) ? b.lda : 1;
+    const T *pa = A + ((b.opA == TKB_OP_N) ? b.offA + i : b.offA + i * b.lda);
+    T *pc = C + b.offC + i;
+    T a[D];
 #pragma unroll
-    for (int j = 0; j < kSkinnyMax; ++j) acc[j] = zero(T{});
-    if (tk.kind == 0) {
-      for (int l = 0; l < k; ++l) {
-        const int64_t ia = (b.opA == TKB_OP_N) ? b.offA + i + (int64_t)l * b.lda : b.offA + l + i * b.lda;
-        const T a = ldA<T>(A + ia, b.opA == TKB_OP_C);
+    for (int l = 0; l < D; ++l) a[l] = (l < kk) ? ldA<T>(pa + l * sa_l, conjA) : zero(T{});
+    T acc[D];
+    if constexpr (BZ) {
 #pragma unroll
-        for (int j = 0; j < kSkinnyMax; ++j)
-          if (j < n) acc[j] = mac(a, Bs[l + j * kSkinnyMax], acc[j]);
+      for (int j = 0; j < D; ++j) acc[j] = zero(T{});
+    } else {
+#pragma unroll
+      for (int j = 0; j < D; ++j) acc[j] = (j < n) ? pc[(int64_t)j * b.ldc] : zero(T{});
+#pragma unroll
+      for (int j = 0; j < D; ++j) acc[j] = mac(acc[j], make_beta<T>(beta), zero(T{}));
+    }
+    // acc += (α·a_l)·op(B)_lj
+#pragma unroll
+    for (int l = 0; l < D; ++l) {
+      if (l < kk) {
+        const T al = scl(a[l], alpha);
+#pragma unroll
+        for (int j = 0; j < D; ++j)
+          if (j < n) acc[j] = mac(al, Bs[l + j * D], acc[j]);
       }
     }
 #pragma unroll
-    for (int j = 0; j < kSkinnyMax; ++j) {
-      if (j < n) {
-        T *p = C + b.offC + i + (int64_t)j * b.ldc;
-        T r = scl(acc[j], alpha);
-        if (!bz) r = mac(*p, make_beta<T>(beta), r);
-        *p = r;
-      }
-    }
+    for (int j = 0; j < D; ++j)
+      if (j < n) pc[(int64_t)j * b.ldc] = acc[j];
   }
 }
 
@@ -422,12 +436,26 @@ int tkb_gemm_skinny_launch(tkb_ctx *ctx, const tkb_plan *p, void *C, const void 
   if (p->nsk == 0) return TKB_OK;
   const int grid = (int)std::min<int64_t>(p->nsk, (int64_t)ctx->num_sms * 8);
   const CDbl a{alpha.re, alpha.im}, bb{beta.re, beta.im};
-  if (p->dtype == TKB_F64)
-    gemm_skinny_kernel<double><<<grid, kSkinnyRows, 0, ctx->stream>>>(
-        p->blocks, p->sktasks, p->nsk, (double *)C, (const double *)A, (const double *)B, a, bb);
-  else
-    gemm_skinny_kernel<double2><<<grid, kSkinnyRows, 0, ctx->stream>>>(
-        p->blocks, p->sktasks, p->nsk, (double2 *)C, (const double2 *)A, (const double2 *)B, a, bb);
+  const bool bz = beta.re == 0.0 && beta.im == 0.0;
+  const int dsel = p->sk_dim <= 4 ? 0 : p->sk_dim <= 8 ? 1 : 2;
+  if (p->dtype == TKB_F64) {
+    using K = void (*)(const GBlock *, const GTile *, int64_t, double *, const double *, const double *, CDbl, CDbl);
+    const K ks[2][3] = {{gemm_skinny_kernel<double, false, 4>, gemm_skinny_kernel<double, false, 8>,
+                         gemm_skinny_kernel<double, false, 16>},
+                        {gemm_skinny_kernel<double, true, 4>, gemm_skinny_kernel<double, true, 8>,
+                         gemm_skinny_kernel<double, true, 16>}};
+    ks[bz][dsel]<<<grid, kSkinnyRows, 0, ctx->stream>>>(p->blocks, p->sktasks, p->nsk, (double *)C,
+                                                        (const double *)A, (const double *)B, a, bb);
+  } else {
+    using K = void (*)(const GBlock *, const GTile *, int64_t, double2 *, const double2 *, const double2 *, CDbl,
+                       CDbl);
+    const K ks[2][3] = {{gemm_skinny_kernel<double2, false, 4>, gemm_skinny_kernel<double2, false, 8>,
+                         gemm_skinny_kernel<double2, false, 16>},
+                        {gemm_skinny_kernel<double2, true, 4>, gemm_skinny_kernel<double2, true, 8>,
+                         gemm_skinny_kernel<double2, true, 16>}};
+    ks[bz][dsel]<<<grid, kSkinnyRows, 0, ctx->stream>>>(p->blocks, p->sktasks, p->nsk, (double2 *)C,
+                                                        (const double2 *)A, (const double2 *)B, a, bb);
+  }
   ctx->launches++;
   TKB_CUDA_TRY(ctx, cudaGetLastError());
   return TKB_OK;

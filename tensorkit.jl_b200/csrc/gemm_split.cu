@@ -7,13 +7,15 @@
 // each slice being the truncated next 7 bits (the subtraction of the integer part is exact
 // in FP64). Columns of op(B) are cut the same way with exponents f_j. Then
 //     C_ij ≈ 2^(e_i+f_j) Σ_{d=2..S+1} 2^-7d P_d,ij ,   P_d = Σ_{s+t=d} a^(s) b^(t),
-// where every P_d is an exact INT32 tensor-core accumulation (k·S·127² < 2^31). Terms with
+// where every P_d is an exact INT32 tensor-core accumulation (K ranges of at most
+// (2^31 − 1)/(S·127²) per product task keep it exact; longer K loops are split). Terms with
 // s+t > S+1 are below the truncation error and dropped. The recombination, the α/β update
 // and everything after the integer products are FP64.
 //
 // ComplexF64 blocks are mapped to one real product: op(A) becomes the 2m×2k real matrix with
 // row pairs (2r, 2r+1) = ([Re A_r, -Im A_r], [Im A_r, Re A_r]) and op(B) the 2k×n matrix
-// [Re B; Im B], so rows 2r and 2r+1 of the real result are Re and Im of C_r.
+// [Re B; Im B], so rows 2r and 2r+1 of the real result are Re and Im of C_r. The two K
+// halves are each zero-padded to round_up(k, 16) positions.
 //
 // Slice layout in the workspace: per block, per slice, the rows of op(A) (op(B)ᵀ) are cut
 // into panels of 128 (64) rows; a panel is a sequence of 32-byte K stages (one tensor-core
@@ -22,11 +24,12 @@
 // bytes between the two 16-byte K chunks). One stage of one slice is therefore one
 // contiguous 4 KiB (2 KiB) block that a single bulk copy moves into shared memory.
 //
-// Launches: exponent pass + slice pass (warp tasks of 32 rows × 64 K) + product pass:
+// Launches: slicing pass (one thread-block cluster per 32 source rows: row maxima,
+// exponents, slices) + product pass:
 //   tcgen05 kernel (default): one CTA per 128×64 output tile (and K range, when the K loop
 //   is split across CTAs); one thread streams the S slice stages of A and B with
-//   cp.async.bulk into a four-stage shared-memory ring and issues tcgen05.mma.kind::i8
-//   (M=128, N=64, K=32) into S int32 accumulators held in tensor memory (S·64 of 512
+//   cp.async.bulk into a shared-memory ring as deep as fits (5 stages at S = 7) and issues
+//   tcgen05.mma.kind::i8 (M=128, N=64, K=32) into S int32 accumulators held in tensor memory (S·64 of 512
 //   columns); four warps read the accumulators back with tcgen05.ld and recombine them in
 //   FP64.
 //   mma.sync kernel (TKB_SPLIT_KERNEL=mma): the same products with int8 mma.sync.
@@ -42,247 +45,381 @@ namespace {
 
 constexpr int PANEL_A = 128, PANEL_B = 64;   // rows per panel
 constexpr int KSTAGE = 32;                   // bytes of K per stage (one tensor-core K step)
-constexpr int NSTAGE = 4;                    // depth of the shared-memory ring
+constexpr int kSmemMax = 232448;             // dynamic shared memory per CTA (227 KiB)
+// depth of the shared-memory ring: as many stages of S slices of A and B as fit, at most 8
+__host__ __device__ constexpr int ring_stages(int S) {
+  return (kSmemMax - 512) / (S * (PANEL_A + PANEL_B) * KSTAGE) < 8
+             ? (kSmemMax - 512) / (S * (PANEL_A + PANEL_B) * KSTAGE)
+             : 8;
+}
 constexpr int SMAX = 7;
-
-struct SliceJob {
-  int32_t block;
-  int32_t operand;  // 0 = rows of op(A), 1 = columns of op(B)
-};
 
 struct CDbl {
   double x, y;
 };
 
-// byte offset of (row r, K byte kb) inside one slice plane
+// 2^e as a double for e in the normal range (exact)
+__device__ __forceinline__ double pow2i(int e) { return __longlong_as_double((long long)(1023 + e) << 52); }
+// out of line: the rare exponents outside the normal range must not inflate the code of the
+// short-lived kernels that scale every element
+__device__ __noinline__ double ldexp_slow(double v, int e) { return ldexp(v, e); }
+// v·2^e: one exact multiplication when 2^e is a normal number, else ldexp
+__device__ __forceinline__ double scale2(double v, int e) {
+  return (e >= -1022 && e <= 1023) ? v * pow2i(e) : ldexp_slow(v, e);
+}
+// exact int64 → double for |x| < 2^51: x is added to the mantissa of 1.5·2^52 (whose unit in
+// the last place is 1), and 1.5·2^52 is subtracted again
+__device__ __forceinline__ double i2d_small(int64_t x) {
+  return __longlong_as_double(x + 0x4338000000000000ll) - 6755399441055744.0;
+}
+
+// byte offset of (row r, K byte kb) inside one slice plane (pr: rows per panel, 64 or 128)
 __host__ __device__ __forceinline__ int64_t slice_off(int64_t r, int64_t kb, int64_t kpad, int pr) {
-  const int64_t panel = r / pr, rr = r % pr;
+  const int lpr = pr == 128 ? 7 : 6;
+  const int64_t panel = r >> lpr, rr = r & (pr - 1);
   const int64_t stg = kb >> 5, kk = kb & 31;
   return panel * (pr * kpad) + stg * (pr * KSTAGE) + (rr >> 3) * 256 + (kk >> 4) * 128 +
          (rr & 7) * 16 + (kk & 15);
 }
 
-// element (r, l) of the logical real operand (rows r of M' or N', column l of K')
-__device__ __forceinline__ double op_elem(const GBlock &b, int operand, int cplx,
-                                          const double *X, int64_t r, int64_t l) {
-  if (operand == 0) {
-    if (!cplx) {
-      const int64_t idx = (b.opA == TKB_OP_N) ? b.offA + r + l * b.lda : b.offA + l + r * b.lda;
-      return X[idx];
-    }
-    const int64_t rr = r >> 1;
-    const bool odd = r & 1;
-    const bool second = l >= b.k;
-    const int64_t ll = second ? l - b.k : l;
-    const int64_t idx = (b.opA == TKB_OP_N) ? b.offA + rr + ll * b.lda : b.offA + ll + rr * b.lda;
-    const double re = X[2 * idx];
-    double im = X[2 * idx + 1];
-    if (b.opA == TKB_OP_C) im = -im;
-    if (!odd) return second ? -im : re;  // row 2r:   [Re, -Im]
-    return second ? re : im;             // row 2r+1: [Im,  Re]
-  }
-  if (!cplx) {
-    const int64_t idx = (b.opB == TKB_OP_N) ? b.offB + l + r * b.ldb : b.offB + r + l * b.ldb;
-    return X[idx];
-  }
-  const bool second = l >= b.k;
-  const int64_t ll = second ? l - b.k : l;
-  const int64_t idx = (b.opB == TKB_OP_N) ? b.offB + ll + r * b.ldb : b.offB + r + ll * b.ldb;
-  if (!second) return X[2 * idx];
-  const double im = X[2 * idx + 1];
-  return (b.opB == TKB_OP_C) ? -im : im;
-}
-
-// Slicing of the operands, in two launches over fine-grained warp tasks. A task is one
-// group of 32 operand rows × one chunk of 128 K positions (rows of all jobs enumerated
-// through the task prefix sums; padding rows and padding K included, so the padded
-// slices are written as zeros).
-//   expo_kernel : per task the partial row maxima, folded into the row exponents with an
-//                 integer atomicMax (the exponent array starts at a very negative value,
-//                 byte 0x80 everywhere); complex row pairs fold into both rows.
-//   slice_kernel: per task the S slices of every element, packed into 16-byte (row-
-//                 contiguous operands, lane = row) or 4-byte (lane = 4 consecutive K)
-//                 stores in the tensor-core operand layout.
-// Row-contiguous operands are real op(A) = A and real op(B) = Bᵀ (consecutive rows are
-// consecutive addresses); the others read 4 consecutive K positions per lane.
-constexpr int KCHUNK = 64;
-
-struct TaskLoc {
-  SliceJob job;
-  int64_t r0, l0;
+// Slicing pass: one task = 32 source rows of one operand of one block over the whole K range,
+// run by a thread-block cluster of 1, 2 or 4 CTAs that split the K range (the partial row
+// maxima are combined through distributed shared memory). Source rows are the rows of op(A)
+// and the columns of op(B) (for ComplexF64 a complex source row of op(A) gives the real row
+// pair 2r, 2r+1). The cluster first reduces the row maxima (phase 1), derives the row
+// exponents, then re-reads the rows (now cached) and writes the S slices (phase 2) as 16-byte
+// chunks of 16 consecutive K of one row in the tensor-core operand layout.
+//
+// Every warp works on warp tiles; after loading, each lane holds 16 consecutive K values of
+// one source row:
+//   rows contiguous in memory (real op(A) = A, op(B) = Bᵀ; complex likewise): lane = row,
+//     tile = 32 rows × 16 K, loads straight from global memory (coalesced along rows);
+//   K contiguous (op(A) = Aᵀ/Aᴴ, op(B) = B): lanes along K (coalesced), staged through a
+//     per-warp shared-memory tile (one padding element per 16) and read back row-wise:
+//     real 4 rows × 128 K, complex 8 rows × 64 K.
+// ComplexF64 K is laid out as [Re | Im] halves of kh = round_up(k, 16) positions each, so a
+// 16-K chunk of the source maps to one chunk in each half.
+struct SliceTask {
+  int32_t block;
+  int32_t operand;  // 0 = rows of op(A), 1 = columns of op(B)
+  int32_t r0;       // first source row
+  int32_t kfull;    // padded source K (real: kpad; complex: kpad / 2), for ordering
 };
 
-__device__ __forceinline__ TaskLoc locate_task(int64_t t, const int64_t *__restrict__ task_begin,
-                                               const SliceJob *__restrict__ jobs, int njobs,
-                                               const GBlock *__restrict__ blocks) {
-  int lo = 0, hi = njobs - 1;
-  while (lo < hi) {
-    const int mid = (lo + hi + 1) >> 1;
-    if (task_begin[mid] <= t) lo = mid; else hi = mid - 1;
-  }
-  const SliceJob job = jobs[lo];
-  const GBlock &b = blocks[job.block];
-  const int64_t nkc = (b.kpad + KCHUNK - 1) / KCHUNK;
-  const int64_t rel = t - task_begin[lo];
-  return TaskLoc{job, (rel / nkc) * 32, (rel % nkc) * KCHUNK};
-}
+constexpr int kSliceThreads = 256;
+constexpr int kSliceWarpSmem = 8 * 68 * 16;  // bytes of one warp's staging tile (complex; real: half)
 
-__device__ __forceinline__ bool row_contiguous(const GBlock &b, int op, int cplx) {
-  return !cplx && ((op == 0 && b.opA == TKB_OP_N) || (op == 1 && b.opB != TKB_OP_N));
-}
+template <bool CPLX>
+struct SrcVal;
+template <>
+struct SrcVal<false> {
+  using T = double;
+};
+template <>
+struct SrcVal<true> {
+  using T = double2;
+};
 
-__global__ void __launch_bounds__(256)
-    expo_kernel(const GBlock *__restrict__ blocks, const int64_t *__restrict__ task_begin,
-                const SliceJob *__restrict__ jobs, int njobs, int64_t ntasks, int cplx,
-                const double *__restrict__ A, const double *__restrict__ B, int8_t *ws) {
-  const int lane = threadIdx.x & 31;
-  const int64_t nw = (int64_t)gridDim.x * (blockDim.x >> 5);
-  for (int64_t t = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); t < ntasks; t += nw) {
-    const TaskLoc L = locate_task(t, task_begin, jobs, njobs, blocks);
-    const GBlock &b = blocks[L.job.block];
-    const int op = L.job.operand;
-    const int64_t Mlog = op == 0 ? (cplx ? 2 * b.m : b.m) : b.n;
-    const int64_t Klog = cplx ? 2 * b.k : b.k;
-    int32_t *expo = reinterpret_cast<int32_t *>(ws + (op == 0 ? b.wsEA : b.wsEB));
-    const double *X = op == 0 ? A : B;
-    const int64_t l1 = min(L.l0 + KCHUNK, Klog);
-    if (row_contiguous(b, op, cplx)) {
-      const int64_t xo = op == 0 ? b.offA : b.offB;
-      const int64_t ld = op == 0 ? b.lda : b.ldb;
-      const int64_t r = L.r0 + lane;
-      if (r >= Mlog || L.l0 >= l1) continue;
-      double mx = 0.0;
-      for (int64_t c = L.l0; c < l1; c += 16) {
-        double v[16];
+__device__ __forceinline__ double zero_of(double) { return 0.0; }
+__device__ __forceinline__ double2 zero_of(double2) { return make_double2(0.0, 0.0); }
+__device__ __forceinline__ double absmax(double v) { return fabs(v); }
+__device__ __forceinline__ double absmax(double2 v) { return fmax(fabs(v.x), fabs(v.y)); }
+
+// Loads warp tile t into v[16]; returns the lane's source row (relative to the task) and the
+// source K of v[0] through row/c; false when the lane's chunk lies beyond the padded K.
+template <bool CPLX, bool ROWC>
+__device__ __forceinline__ bool load_tile(int t, const typename SrcVal<CPLX>::T *__restrict__ X,
+                                          int64_t xo, int64_t rs, int64_t ks, int64_t r0,
+                                          int64_t msrc, int64_t ksrc, int64_t kfull,
+                                          typename SrcVal<CPLX>::T *stage, int lane,
+                                          typename SrcVal<CPLX>::T (&v)[16], int &row, int64_t &c) {
+  using T = typename SrcVal<CPLX>::T;
+  const T z = zero_of(T{});
+  if constexpr (ROWC) {
+    row = lane;
+    c = 16 * (int64_t)t;
+    const int64_t r = r0 + lane;
+    const bool rv = r < msrc;
+    const T *p = X + xo + r * rs;
 #pragma unroll
-        for (int q = 0; q < 16; ++q) v[q] = (c + q < l1) ? X[xo + r + (c + q) * ld] : 0.0;
+    for (int q = 0; q < 16; ++q) v[q] = (rv && c + q < ksrc) ? __ldg(p + (c + q) * ks) : z;
+    return true;
+  } else {
+    constexpr int RG = CPLX ? 8 : 4;       // rows per warp tile
+    constexpr int KW = CPLX ? 64 : 128;    // K per warp tile
+    constexpr int NH = KW / 32;            // loads per row per lane
+    constexpr int RP = (KW / 16) * 17;     // staging row pitch (elements)
+    const int ngrp = 32 / RG;
+    const int grp = t % ngrp;
+    const int64_t k0 = (int64_t)(t / ngrp) * KW;
+    T tmp[RG * NH];
 #pragma unroll
-        for (int q = 0; q < 16; ++q) mx = fmax(mx, fabs(v[q]));
-      }
-      if (mx > 0.0) {
-        int e;
-        frexp(mx, &e);
-        atomicMax(&expo[r], e);
-      }
-      continue;
-    }
-    // lane = 2 consecutive K positions; 8 rows per batch so 16 loads are in flight per lane
-    for (int rb = 0; rb < 32; rb += 8) {
-      double mx[8];
+    for (int rr = 0; rr < RG; ++rr) {
+      const int64_t r = r0 + grp * RG + rr;
+      const bool rv = r < msrc;
+      const T *p = X + xo + r * rs;
 #pragma unroll
-      for (int rr = 0; rr < 8; ++rr) {
-        const int64_t r = L.r0 + rb + rr;
-        mx[rr] = 0.0;
-#pragma unroll
-        for (int q = 0; q < 2; ++q) {
-          const int64_t l = L.l0 + 2 * lane + q;
-          if (r < Mlog && l < l1) mx[rr] = fmax(mx[rr], fabs(op_elem(b, op, cplx, X, r, l)));
-        }
-      }
-#pragma unroll
-      for (int rr = 0; rr < 8; ++rr) {
-        const int64_t r = L.r0 + rb + rr;
-        double m = mx[rr];
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
-        if (lane == 0 && r < Mlog && m > 0.0) {
-          int e;
-          frexp(m, &e);
-          atomicMax(&expo[r], e);
-          if (cplx && op == 0) atomicMax(&expo[r ^ 1], e);  // a complex row pair shares one exponent
-        }
+      for (int h = 0; h < NH; ++h) {
+        const int64_t l = k0 + 32 * h + lane;
+        tmp[rr * NH + h] = (rv && l < ksrc) ? __ldg(p + l) : z;
       }
     }
-  }
-}
-
-template <int S>
-__device__ __forceinline__ void cut(double x, uint32_t (&w)[S], int shift) {
+    __syncwarp();
 #pragma unroll
-  for (int s = 0; s < S; ++s) {
-    x *= 128.0;
-    const double qd = trunc(x);
-    x -= qd;
-    w[s] |= ((uint32_t)(uint8_t)(int8_t)qd) << shift;
+    for (int rr = 0; rr < RG; ++rr)
+#pragma unroll
+      for (int h = 0; h < NH; ++h) stage[rr * RP + (2 * h + (lane >> 4)) * 17 + (lane & 15)] = tmp[rr * NH + h];
+    __syncwarp();
+    constexpr int LPR = 32 / RG;  // lanes per row
+    const int rr = lane / LPR, kap = lane % LPR;
+#pragma unroll
+    for (int q = 0; q < 16; ++q) v[q] = stage[rr * RP + kap * 17 + q];
+    row = grp * RG + rr;
+    c = k0 + 16 * kap;
+    return c < kfull;
   }
 }
 
+// Integer slicing. For a row with exponent e (every |v| < 2^e), Y = floor(|v|·2^(7S−e)) < 2^(7S)
+// comes straight from the bits of v: v = ±m·2^(E−1075) (normal; subnormal: E = 1, no hidden
+// bit), so Y = m >> (e − 7S + 1075 − E), a right shift of at least 53 − 7S ≥ 4 bits when v is
+// normal. The S slices are the base-128 digits of Y, most significant first, each carrying
+// the sign of v: exactly the digits of S rounds of (y ← 128·y, q ← trunc(y), y ← y − q) on
+// y = v·2^−e, so the dropped low-order products keep random signs (no bias across K).
+struct Fixed {
+  uint32_t hi;  // Y >> 28
+  uint32_t lo;  // Y mod 2^28
+};
 template <int S>
-__global__ void __launch_bounds__(256)
-    slice_kernel(const GBlock *__restrict__ blocks, const int64_t *__restrict__ task_begin,
-                 const SliceJob *__restrict__ jobs, int njobs, int64_t ntasks, int cplx,
+__device__ __forceinline__ Fixed to_fixed(double v, int e, bool &neg) {
+  const uint64_t bits = (uint64_t)__double_as_longlong(v);
+  const int E = (int)((bits >> 52) & 0x7ff);
+  uint64_t m = bits & 0xfffffffffffffull;
+  int Ee = 1;
+  if (E != 0) {
+    m |= 1ull << 52;
+    Ee = E;
+  }
+  const int sh = e - 7 * S + 1075 - Ee;  // < 0 only for rows whose maximum is subnormal
+  const uint64_t y = sh >= 64 ? 0ull : sh >= 0 ? (m >> sh) : (m << -sh);
+  neg = (bits >> 63) != 0;
+  return Fixed{(uint32_t)(y >> 28), (uint32_t)y & 0xfffffffu};
+}
+// byte masks of the negative values among 16 (0xff per negative value, 4 words)
+__device__ __forceinline__ void sign_masks(const bool (&neg)[16], uint32_t (&M)[4]) {
+#pragma unroll
+  for (int h = 0; h < 4; ++h) {
+    uint32_t m = 0u;
+#pragma unroll
+    for (int b = 0; b < 4; ++b) m |= (neg[4 * h + b] ? 0xffu : 0u) << (8 * b);
+    M[h] = m;
+  }
+}
+// digit sl (0 = most significant) of 16 fixed-point values as one 16-byte chunk of int8:
+// the 7-bit digit of Y, negated in the bytes that M marks (bytes 0..127: the negation is
+// (0x80 − b) ^ 0x80, with no carry between bytes)
+template <int S>
+__device__ __forceinline__ uint4 slice16(const Fixed (&x)[16], const uint32_t (&M)[4], int sl) {
+  const int sh = 7 * (S - 1 - sl);
+  uint32_t d[16];
+  if (sh >= 28) {
+#pragma unroll
+    for (int q = 0; q < 16; ++q) d[q] = x[q].hi >> (sh - 28);
+  } else {
+#pragma unroll
+    for (int q = 0; q < 16; ++q) d[q] = (x[q].lo >> sh) | (x[q].hi << (28 - sh));
+  }
+  uint32_t w[4];
+#pragma unroll
+  for (int h = 0; h < 4; ++h) {
+    const uint32_t u = __byte_perm(__byte_perm(d[4 * h], d[4 * h + 1], 0x0040),
+                                   __byte_perm(d[4 * h + 2], d[4 * h + 3], 0x0040), 0x5410) & 0x7f7f7f7fu;
+    const uint32_t n = (0x80808080u - u) ^ 0x80808080u;
+    w[h] = (u & ~M[h]) | (n & M[h]);
+  }
+  return make_uint4(w[0], w[1], w[2], w[3]);
+}
+
+// thread-block cluster helpers (the K range of a task is split over the CTAs of a cluster)
+__device__ __forceinline__ uint32_t cluster_rank() {
+  uint32_t r;
+  asm volatile("mov.u32 %0, %%cluster_ctarank;\n" : "=r"(r));
+  return r;
+}
+__device__ __forceinline__ uint32_t cluster_size() {
+  uint32_t r;
+  asm volatile("mov.u32 %0, %%cluster_nctarank;\n" : "=r"(r));
+  return r;
+}
+__device__ __forceinline__ void cluster_arrive() {
+  asm volatile("barrier.cluster.arrive.release.aligned;\n" ::: "memory");
+}
+__device__ __forceinline__ void cluster_wait() {
+  asm volatile("barrier.cluster.wait.acquire.aligned;\n" ::: "memory");
+}
+// 64-bit load from the shared memory of CTA `rank` of this cluster, at the address that `p`
+// has in this CTA
+__device__ __forceinline__ unsigned long long ld_dsmem_u64(const void *p, uint32_t rank) {
+  uint32_t remote;
+  asm volatile("mapa.shared::cluster.u32 %0, %1, %2;\n"
+               : "=r"(remote)
+               : "r"((uint32_t)__cvta_generic_to_shared(p)), "r"(rank));
+  unsigned long long v;
+  asm volatile("ld.shared::cluster.u64 %0, [%1];\n" : "=l"(v) : "r"(remote) : "memory");
+  return v;
+}
+
+template <int S, bool CPLX, bool ROWC>
+__device__ __forceinline__ void slice_task(const GBlock &b, int op, int64_t r0, const void *Xv, int8_t *ws,
+                                           unsigned char *wsmem, unsigned long long *rmax, int *rexp) {
+  using T = typename SrcVal<CPLX>::T;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  // the CTAs of a cluster share the task's warp tiles: crank·8 + warp, then every 8·csize
+  const uint32_t crank = cluster_rank(), csize = cluster_size();
+  const int t0 = (int)crank * (kSliceThreads / 32) + warp;
+  const int tstep = (int)csize * (kSliceThreads / 32);
+  const T *X = reinterpret_cast<const T *>(Xv);
+  T *stage = reinterpret_cast<T *>(wsmem + warp * (CPLX ? kSliceWarpSmem : kSliceWarpSmem / 2));
+  const int64_t xo = op == 0 ? b.offA : b.offB;
+  const int opx = op == 0 ? b.opA : b.opB;
+  // strides of source rows and K in elements
+  int64_t rs, ks;
+  if (op == 0) {
+    rs = opx == TKB_OP_N ? 1 : b.lda;
+    ks = opx == TKB_OP_N ? b.lda : 1;
+  } else {
+    rs = opx == TKB_OP_N ? b.ldb : 1;
+    ks = opx == TKB_OP_N ? 1 : b.ldb;
+  }
+  const bool conj = opx == TKB_OP_C;
+  const int64_t msrc = op == 0 ? b.m : b.n;
+  const int64_t kfull = CPLX ? b.kpad / 2 : b.kpad;
+  const int ntile = ROWC ? (int)(kfull / 16)
+                         : (CPLX ? 4 : 8) * (int)((kfull + (CPLX ? 63 : 127)) / (CPLX ? 64 : 128));
+
+  // phase 1: row maxima of this CTA's tiles
+  for (int t = t0; t < ntile; t += tstep) {
+    T v[16];
+    int row;
+    int64_t c;
+    load_tile<CPLX, ROWC>(t, X, xo, rs, ks, r0, msrc, b.k, kfull, stage, lane, v, row, c);
+    double m = 0.0;
+#pragma unroll
+    for (int q = 0; q < 16; ++q) m = fmax(m, absmax(v[q]));
+    if (m > 0.0) atomicMax(&rmax[row], (unsigned long long)__double_as_longlong(m));
+  }
+  // partial maxima of the cluster's CTAs → row exponents (written by CTA 0)
+  __syncthreads();
+  cluster_arrive();
+  cluster_wait();
+  if (tid < 32) {
+    unsigned long long mb = rmax[tid];
+    for (uint32_t q = 0; q < csize; ++q)
+      if (q != crank) mb = max(mb, ld_dsmem_u64(&rmax[tid], q));
+    const double m = __longlong_as_double((long long)mb);
+    int e = 0;
+    if (m > 0.0) frexp(m, &e);
+    rexp[tid] = e;
+    int32_t *ex = reinterpret_cast<int32_t *>(ws + (op == 0 ? b.wsEA : b.wsEB));
+    const int64_t r = r0 + tid;
+    if (crank == 0) {
+      if (CPLX && op == 0) {
+        ex[2 * r] = e;
+        ex[2 * r + 1] = e;
+      } else {
+        ex[r] = e;
+      }
+    }
+  }
+  // done reading the peers' maxima; the matching wait before exit keeps every CTA's shared
+  // memory alive until all peers have read it
+  cluster_arrive();
+  __syncthreads();
+
+  // phase 2: slices
+  const int pr = op == 0 ? PANEL_A : PANEL_B;
+  const int64_t kpad = b.kpad;
+  int8_t *base = ws + (op == 0 ? b.wsA : b.wsB);
+  const int64_t plane = (int64_t)(op == 0 ? b.mpad : b.npad) * kpad;
+  for (int t = t0; t < ntile; t += tstep) {
+    T v[16];
+    int row;
+    int64_t c;
+    const bool ok = load_tile<CPLX, ROWC>(t, X, xo, rs, ks, r0, msrc, b.k, kfull, stage, lane, v, row, c);
+    if (!ok) continue;
+    const int e = rexp[row];
+    const int64_t r = r0 + row;
+    // one slice per iteration (not unrolled: the body is reused S times, which keeps the
+    // code of this short-lived kernel small)
+    if constexpr (!CPLX) {
+      Fixed x[16];
+      bool ng[16];
+      uint32_t M[4];
+#pragma unroll
+      for (int q = 0; q < 16; ++q) x[q] = to_fixed<S>(v[q], e, ng[q]);
+      sign_masks(ng, M);
+      int8_t *p = base + slice_off(r, c, kpad, pr);
+#pragma unroll 1
+      for (int sl = 0; sl < S; ++sl, p += plane) *reinterpret_cast<uint4 *>(p) = slice16<S>(x, M, sl);
+    } else {
+      Fixed xr[16], xi[16];
+      bool nr[16], ni[16];
+      uint32_t Mr[4], Mi[4], Mn[4];
+#pragma unroll
+      for (int q = 0; q < 16; ++q) {
+        xr[q] = to_fixed<S>(v[q].x, e, nr[q]);
+        xi[q] = to_fixed<S>(conj ? -v[q].y : v[q].y, e, ni[q]);
+      }
+      sign_masks(nr, Mr);
+      sign_masks(ni, Mi);
+      if (op == 0) {  // rows 2r: [Re | -Im], 2r+1: [Im | Re]
+#pragma unroll
+        for (int h = 0; h < 4; ++h) Mn[h] = ~Mi[h];
+        int8_t *p0 = base + slice_off(2 * r, c, kpad, pr);
+        int8_t *p1 = base + slice_off(2 * r, kfull + c, kpad, pr);
+        int8_t *p2 = base + slice_off(2 * r + 1, c, kpad, pr);
+        int8_t *p3 = base + slice_off(2 * r + 1, kfull + c, kpad, pr);
+#pragma unroll 1
+        for (int sl = 0; sl < S; ++sl) {
+          const uint4 ur = slice16<S>(xr, Mr, sl);
+          const int64_t o = sl * plane;
+          *reinterpret_cast<uint4 *>(p0 + o) = ur;
+          *reinterpret_cast<uint4 *>(p1 + o) = slice16<S>(xi, Mn, sl);
+          *reinterpret_cast<uint4 *>(p2 + o) = slice16<S>(xi, Mi, sl);
+          *reinterpret_cast<uint4 *>(p3 + o) = ur;
+        }
+      } else {        // column j of op(B): [Re | Im]
+        int8_t *p0 = base + slice_off(r, c, kpad, pr);
+        int8_t *p1 = base + slice_off(r, kfull + c, kpad, pr);
+#pragma unroll 1
+        for (int sl = 0; sl < S; ++sl) {
+          const int64_t o = sl * plane;
+          *reinterpret_cast<uint4 *>(p0 + o) = slice16<S>(xr, Mr, sl);
+          *reinterpret_cast<uint4 *>(p1 + o) = slice16<S>(xi, Mi, sl);
+        }
+      }
+    }
+  }
+  cluster_wait();
+}
+
+template <int S, bool CPLX>
+__global__ void __launch_bounds__(kSliceThreads, CPLX ? 1 : 2)
+    slice_kernel(const GBlock *__restrict__ blocks, const SliceTask *__restrict__ tasks,
                  const double *__restrict__ A, const double *__restrict__ B, int8_t *ws) {
-  const int lane = threadIdx.x & 31;
-  const int64_t nw = (int64_t)gridDim.x * (blockDim.x >> 5);
-  for (int64_t t = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); t < ntasks; t += nw) {
-    const TaskLoc L = locate_task(t, task_begin, jobs, njobs, blocks);
-    const GBlock &b = blocks[L.job.block];
-    const int op = L.job.operand;
-    const int64_t Mlog = op == 0 ? (cplx ? 2 * b.m : b.m) : b.n;
-    const int64_t Klog = cplx ? 2 * b.k : b.k;
-    const int64_t rows_pad = op == 0 ? b.mpad : b.npad;
-    const int pr = op == 0 ? PANEL_A : PANEL_B;
-    const int64_t kpad = b.kpad;
-    int8_t *base = ws + (op == 0 ? b.wsA : b.wsB);
-    const int32_t *expo = reinterpret_cast<const int32_t *>(ws + (op == 0 ? b.wsEA : b.wsEB));
-    const double *X = op == 0 ? A : B;
-    const int64_t plane = rows_pad * kpad;
-    const int64_t l1 = min(L.l0 + KCHUNK, kpad);
-    if (row_contiguous(b, op, cplx)) {
-      const int64_t xo = op == 0 ? b.offA : b.offB;
-      const int64_t ld = op == 0 ? b.lda : b.ldb;
-      const int64_t r = L.r0 + lane;
-      const bool valid = r < Mlog;
-      const int e = valid ? max(expo[r], -1100) : 0;
-      for (int64_t c = L.l0; c < l1; c += 16) {
-        uint32_t w[4][S];
-#pragma unroll
-        for (int h = 0; h < 4; ++h)
-#pragma unroll
-          for (int s = 0; s < S; ++s) w[h][s] = 0u;
-        double v[16];
-#pragma unroll
-        for (int q = 0; q < 16; ++q) v[q] = (valid && c + q < Klog) ? X[xo + r + (c + q) * ld] : 0.0;
-#pragma unroll
-        for (int q = 0; q < 16; ++q) cut<S>(ldexp(v[q], -e), w[q >> 2], 8 * (q & 3));
-        const int64_t off = slice_off(r, c, kpad, pr);
-#pragma unroll
-        for (int s = 0; s < S; ++s)
-          *reinterpret_cast<uint4 *>(base + s * plane + off) = make_uint4(w[0][s], w[1][s], w[2][s], w[3][s]);
-      }
-      continue;
-    }
-    // lane = 2 consecutive K positions (64 per warp); 8 rows per batch, loads first
-    const int64_t lb = L.l0 + 2 * lane;
-    for (int rb = 0; rb < 32; rb += 8) {
-      double v[8][2];
-      int ex[8];
-#pragma unroll
-      for (int rr = 0; rr < 8; ++rr) {
-        const int64_t r = L.r0 + rb + rr;
-        const bool valid = r < Mlog;
-        ex[rr] = valid ? max(expo[r], -1100) : 0;
-#pragma unroll
-        for (int q = 0; q < 2; ++q) {
-          const int64_t l = lb + q;
-          v[rr][q] = (valid && l < Klog) ? op_elem(b, op, cplx, X, r, l) : 0.0;
-        }
-      }
-      if (lb >= l1) continue;
-#pragma unroll
-      for (int rr = 0; rr < 8; ++rr) {
-        const int64_t r = L.r0 + rb + rr;
-        uint32_t w[S];
-#pragma unroll
-        for (int s = 0; s < S; ++s) w[s] = 0u;
-#pragma unroll
-        for (int q = 0; q < 2; ++q) cut<S>(ldexp(v[rr][q], -ex[rr]), w, 8 * q);
-        const int64_t off = slice_off(r, lb, kpad, pr);
-#pragma unroll
-        for (int s = 0; s < S; ++s) *reinterpret_cast<uint16_t *>(base + s * plane + off) = (uint16_t)w[s];
-      }
-    }
-  }
+  extern __shared__ __align__(16) unsigned char slice_smem[];
+  __shared__ unsigned long long rmax[32];
+  __shared__ int rexp[32];
+  const SliceTask task = tasks[blockIdx.x / cluster_size()];
+  const GBlock &b = blocks[task.block];
+  const int op = task.operand;
+  if (threadIdx.x < 32) rmax[threadIdx.x] = 0ull;
+  __syncthreads();
+  const int opx = op == 0 ? b.opA : b.opB;
+  const bool rowc = op == 0 ? opx == TKB_OP_N : opx != TKB_OP_N;
+  const void *X = op == 0 ? (const void *)A : (const void *)B;
+  if (rowc) slice_task<S, CPLX, true>(b, op, task.r0, X, ws, slice_smem, rmax, rexp);
+  else slice_task<S, CPLX, false>(b, op, task.r0, X, ws, slice_smem, rmax, rexp);
 }
 
 // ---- shared epilogue: recombine one output value --------------------------------------------
@@ -375,14 +512,22 @@ __device__ __forceinline__ void umma_commit(uint64_t *bar) {
                    smem_u32(bar))
                : "memory");
 }
-__device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&r)[16]) {
+// tcgen05.ld without the wait; tmem_ld_wait on the same registers orders their uses after it
+__device__ __forceinline__ void tmem_ld16_issue(uint32_t taddr, uint32_t (&r)[16]) {
   asm volatile(
       "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, "
       "[%16];\n"
       : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
         "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
       : "r"(taddr));
-  asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+}
+__device__ __forceinline__ void tmem_ld_wait(uint32_t (&r)[16]) {
+  asm volatile("tcgen05.wait::ld.sync.aligned;\n"
+               : "+r"(r[0]), "+r"(r[1]), "+r"(r[2]), "+r"(r[3]), "+r"(r[4]), "+r"(r[5]), "+r"(r[6]),
+                 "+r"(r[7]), "+r"(r[8]), "+r"(r[9]), "+r"(r[10]), "+r"(r[11]), "+r"(r[12]), "+r"(r[13]),
+                 "+r"(r[14]), "+r"(r[15])
+               :
+               : "memory");
 }
 __device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory"); }
 __device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory"); }
@@ -411,11 +556,13 @@ __global__ void __launch_bounds__(128, 1)
   constexpr uint32_t A_BYTES = S * PANEL_A * KSTAGE, B_BYTES = S * PANEL_B * KSTAGE;
   constexpr uint32_t STAGE = A_BYTES + B_BYTES;
   extern __shared__ __align__(1024) unsigned char smem[];
+  constexpr int NSTAGE = ring_stages(S);
   uint64_t *full = reinterpret_cast<uint64_t *>(smem + NSTAGE * STAGE);
   uint64_t *empty = full + NSTAGE;
   uint64_t *done = full + 2 * NSTAGE;
   uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(full + 2 * NSTAGE + 1);
   int *ticket = reinterpret_cast<int *>(full + 2 * NSTAGE + 2);
+  int *ebs = reinterpret_cast<int *>(full + 2 * NSTAGE + 4);  // column exponents of the tile
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const SplitTile tile = tiles[blockIdx.x];
   const GBlock b = blocks[tile.block];
@@ -442,7 +589,14 @@ __global__ void __launch_bounds__(128, 1)
   __syncthreads();
   tc_fence_after();
   const uint32_t tmem = has_k ? *tmem_slot : 0u;
+  if (tid >= 64) {  // column exponents into shared memory while warp 0 starts the products
+    const int col = tid - 64;
+    const int64_t j = tile.n0 + col;
+    ebs[col] = (has_k && j < b.n) ? max(reinterpret_cast<const int32_t *>(ws + b.wsEB)[j], -1100) : 0;
+  }
 
+  // producer: lane 0 of warp 0; the other lanes of warp 0 wait at the __syncwarp below (no
+  // polling that would take issue slots from the producer)
   if (has_k && tid == 0) {
     const int8_t *gA = ws + b.wsA + (int64_t)(tile.m0 / PANEL_A) * PANEL_A * b.kpad;
     const int8_t *gB = ws + b.wsB + (int64_t)(tile.n0 / PANEL_B) * PANEL_B * b.kpad;
@@ -506,73 +660,110 @@ __global__ void __launch_bounds__(128, 1)
       for (int k = consumed; k < issued; ++k) mbar_wait(&full[k % NSTAGE], (k / NSTAGE) & 1);
     }
   }
+  if (warp == 0) __syncwarp();
   if (has_k) {
     if (!mbar_wait(done, 0)) atomicExch(err, 2);
     tc_fence_after();
   }
   __syncwarp();  // tcgen05.ld is warp-collective: reconverge after the divergent waits
+  __syncthreads();  // ebs visible; every warp is past its wait
   // epilogue: warp w owns accumulator rows 32w..32w+31 (TMEM lanes)
   const int32_t *eA = reinterpret_cast<const int32_t *>(ws + b.wsEA);
-  const int32_t *eB = reinterpret_cast<const int32_t *>(ws + b.wsEB);
   const int64_t Mreal = cplx ? 2 * b.m : b.m;
   const int row = 32 * warp + lane;
   const int64_t i = tile.m0 + row;
-  // exponents of all-zero rows stay at the 0x80808080 reset value: clamp before adding
   const int ei = (has_k && i < Mreal) ? max(eA[i], -1100) : 0;
   // this CTA's FP64 recombination of its diagonals: chunk c of 16 columns
   auto recombine = [&](int c, double (&v)[16]) {
 #pragma unroll
     for (int q = 0; q < 16; ++q) v[q] = 0.0;
     if (!has_k) return;
+    // all S loads in flight, then one wait (the first wait covers every load issued before it)
+    uint32_t r[S][16];
 #pragma unroll
-    for (int d = S - 1; d >= 0; --d) {
-      uint32_t r[16];
-      tmem_ld16(tmem + ((uint32_t)(32 * warp) << 16) + (uint32_t)(d * 64 + c * 16), r);
+    for (int d = 0; d < S; ++d)
+      tmem_ld16_issue(tmem + ((uint32_t)(32 * warp) << 16) + (uint32_t)(d * 64 + c * 16), r[d]);
 #pragma unroll
-      for (int q = 0; q < 16; ++q) v[q] += ldexp((double)(int32_t)r[q], -7 * (d + 2));
+    for (int d = 0; d < S; ++d) tmem_ld_wait(r[d]);
+    // exact integer recombination: diagonals d = 0..2, 3..4, 5..6 are combined by Horner's
+    // rule in base 128 into three int64 groups (each below 2^46 in magnitude), each turned
+    // into a double without a conversion instruction, then scaled and summed in FP64
+#pragma unroll
+    for (int q = 0; q < 16; ++q) {
+      int64_t g0 = 0, g1 = 0, g2 = 0;
+#pragma unroll
+      for (int d = 0; d < S; ++d) {
+        const int64_t pd = (int32_t)r[d][q];
+        if (d < 3) g0 = g0 * 128 + pd;
+        else if (d < 5) g1 = g1 * 128 + pd;
+        else g2 = g2 * 128 + pd;
+      }
+      double acc = i2d_small(g0) * pow2i(-7 * ((S < 3 ? S : 3) + 1));
+      if (S > 3) acc = fma(i2d_small(g1), pow2i(-7 * ((S < 5 ? S : 5) + 1)), acc);
+      if (S > 5) acc = fma(i2d_small(g2), pow2i(-7 * (S + 1)), acc);
+      v[q] = acc;
     }
   };
-  bool write_out = true;
-  if (tile.nsplit > 1) {
-    double *mine = part + (int64_t)(tile.pbase + tile.sid) * (64 * 128);  // [col][row]
+  // final values of chunk c: exponent scaling, α/β update, store to C (real: every old
+  // value of C is loaded before the first store, so no load waits behind a store)
+  auto final_store = [&](int c, const double (&v)[16]) {
+    double r[16];
+#pragma unroll
+    for (int q = 0; q < 16; ++q) r[q] = has_k ? scale2(v[q], ei + ebs[c * 16 + q]) : v[q];
+    if (!cplx) {
+      const int64_t j0 = tile.n0 + c * 16;
+      const int nj = (int)min((int64_t)16, b.n - j0);
+      if (i >= b.m || nj <= 0) return;
+      double *pc = C + b.offC + i + j0 * b.ldc;
+      double old[16];
+#pragma unroll
+      for (int q = 0; q < 16; ++q) old[q] = (!bz && q < nj) ? pc[q * b.ldc] : 0.0;
+#pragma unroll
+      for (int q = 0; q < 16; ++q)
+        if (q < nj) pc[q * b.ldc] = bz ? alpha.x * r[q] : fma(beta.x, old[q], alpha.x * r[q]);
+      return;
+    }
+#pragma unroll
+    for (int q = 0; q < 16; ++q) store_out(r[q], i, tile.n0 + c * 16 + q, b, cplx, C, alpha, beta, bz, 1);
+  };
+  bool last = tile.nsplit == 1;
+  double *mine = part + (int64_t)(tile.pbase + tile.sid) * (64 * 128);  // [col][row]
 #pragma unroll 1
-    for (int c = 0; c < 4; ++c) {
-      double v[16];
-      recombine(c, v);
+  for (int c = 0; c < 4; ++c) {
+    double v[16];
+    recombine(c, v);
+    if (last) {
+      final_store(c, v);
+    } else {
 #pragma unroll
       for (int q = 0; q < 16; ++q) __stcg(&mine[(c * 16 + q) * 128 + row], v[q]);
     }
+  }
+  if (!last) {
     __threadfence();
     __syncthreads();
     if (tid == 0) *ticket = atomicAdd(&pcnt[tile.slot], 1);
     __syncthreads();
-    write_out = (*ticket == tile.nsplit - 1);
-    if (write_out) __threadfence();
-  }
-  if (write_out) {
+    if (*ticket == tile.nsplit - 1) {  // the last CTA of the tile adds the partials in split order
+      __threadfence();
 #pragma unroll 1
-    for (int c = 0; c < 4; ++c) {
-      double v[16];
-      if (tile.nsplit > 1) {
+      for (int c = 0; c < 4; ++c) {
+        double v[16];
 #pragma unroll
         for (int q = 0; q < 16; ++q) v[q] = 0.0;
+#pragma unroll 4
         for (int sp = 0; sp < tile.nsplit; ++sp) {
           const double *src = part + (int64_t)(tile.pbase + sp) * (64 * 128);
+          double t[16];
 #pragma unroll
-          for (int q = 0; q < 16; ++q) v[q] += __ldcg(&src[(c * 16 + q) * 128 + row]);
+          for (int q = 0; q < 16; ++q) t[q] = __ldcg(&src[(c * 16 + q) * 128 + row]);
+#pragma unroll
+          for (int q = 0; q < 16; ++q) v[q] += t[q];
         }
-      } else {
-        recombine(c, v);
+        final_store(c, v);
       }
-#pragma unroll
-      for (int q = 0; q < 16; ++q) {
-        const int64_t j = tile.n0 + c * 16 + q;
-        double val = v[q];
-        if (has_k) val = ldexp(val, ei + ((j < b.n) ? max(eB[j], -1100) : 0));
-        store_out(val, i, j, b, cplx, C, alpha, beta, bz, 1);
-      }
+      if (tid == 0) pcnt[tile.slot] = 0;
     }
-    if (tile.nsplit > 1 && tid == 0) pcnt[tile.slot] = 0;
   }
   tc_fence_before();
   __syncthreads();
@@ -715,8 +906,9 @@ __global__ void __launch_bounds__(256)
               double v = 0.0;
               if (tile.kind == 0) {
 #pragma unroll
-                for (int d = S - 1; d >= 0; --d) v += ldexp((double)acc[d][mt][nt][hr * 2 + hc], -7 * (d + 2));
-                v = ldexp(v, ((i < Mreal) ? max(eA[i], -1100) : 0) + ((j < b.n) ? max(eB[j], -1100) : 0));
+                for (int d = S - 1; d >= 0; --d)
+                  v = fma((double)acc[d][mt][nt][hr * 2 + hc], pow2i(-7 * (d + 2)), v);
+                v = scale2(v, ((i < Mreal) ? max(eA[i], -1100) : 0) + ((j < b.n) ? max(eB[j], -1100) : 0));
               }
               store_out(v, i, j, b, cplx, C, alpha, beta, bz, 4);
             }
@@ -743,20 +935,34 @@ template <int S>
 int launch_split(tkb_ctx *ctx, const tkb_plan *p, void *C, const void *A, const void *B, CDbl a, CDbl b) {
   const int cplx = p->dtype == TKB_C128 ? 1 : 0;
   if (p->nsrows > 0) {
-    // one warp per (32-row group, 128-K chunk) task
-    const int grid = (int)std::min<int64_t>((p->nsrows + 7) / 8, (int64_t)ctx->num_sms * 16);
-    int8_t *ws = (int8_t *)ctx->ws;
-    TKB_CUDA_TRY(ctx, cudaMemsetAsync(ws + p->expo_off, 0x80, p->expo_bytes, ctx->stream));
-    expo_kernel<<<grid, 256, 0, ctx->stream>>>(p->blocks, p->srow_begin, (const SliceJob *)p->sjobs,
-                                               p->nsjobs, p->nsrows, cplx, (const double *)A,
-                                               (const double *)B, ws);
-    slice_kernel<S><<<grid, 256, 0, ctx->stream>>>(p->blocks, p->srow_begin, (const SliceJob *)p->sjobs,
-                                                   p->nsjobs, p->nsrows, cplx, (const double *)A,
-                                                   (const double *)B, ws);
-    ctx->launches += 2;
+    // complex tiles stage 16-byte elements: twice the shared memory of real ones
+    const size_t smem = (size_t)(kSliceThreads / 32) * kSliceWarpSmem / (cplx ? 1 : 2);
+    auto k = cplx ? slice_kernel<S, true> : slice_kernel<S, false>;
+    TKB_CUDA_TRY(ctx, cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    // CTAs per task (a thread-block cluster): as many as still fit one wave at two CTAs per SM
+    int cs = 1;
+    while (cs < 4 && p->nsrows * (cs * 2) <= 2 * (int64_t)ctx->num_sms) cs *= 2;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)(p->nsrows * cs));
+    cfg.blockDim = dim3(kSliceThreads);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = ctx->stream;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = cs;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    TKB_CUDA_TRY(ctx, cudaLaunchKernelEx(&cfg, k, (const GBlock *)p->blocks, (const SliceTask *)p->sjobs,
+                                         (const double *)A, (const double *)B, (int8_t *)ctx->ws));
+    ctx->launches++;
     TKB_CUDA_TRY(ctx, cudaGetLastError());
   }
   if (use_mma_sync()) {
+    for (const GBlock &hb : p->hblocks)
+      if (!hb.skinny && (int64_t)hb.kpad * S * 127 * 127 > 2147483647ll)
+        return tkb_set_error(ctx, TKB_ERR_UNSUPPORTED, "mma.sync split kernel: K too long for exact int32 products");
     const size_t smem = 2 * (size_t)(2 * S * SBM * SPITCH);
     auto k = gemm_split_mma_kernel<S>;
     TKB_CUDA_TRY(ctx, cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
@@ -764,7 +970,7 @@ int launch_split(tkb_ctx *ctx, const tkb_plan *p, void *C, const void *A, const 
     k<<<grid, 256, smem, ctx->stream>>>(p->blocks, p->stiles, (int)p->nstiles, ctx->counters,
                                         (const int8_t *)ctx->ws, cplx, (double *)C, a, b);
   } else {
-    const size_t smem = NSTAGE * (size_t)S * (PANEL_A + PANEL_B) * KSTAGE + 128;
+    const size_t smem = ring_stages(S) * (size_t)S * (PANEL_A + PANEL_B) * KSTAGE + 512;
     auto k = gemm_split_tc_kernel<S>;
     TKB_CUDA_TRY(ctx, cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     k<<<(int)p->nkstiles, 128, smem, ctx->stream>>>(p->blocks, (const SplitTile *)p->kstiles,
@@ -787,17 +993,16 @@ int tkb_gemm_split_prepare(tkb_ctx *ctx, tkb_plan *p) {
   if (S < 3 || S > SMAX) return tkb_set_error(ctx, TKB_ERR_UNSUPPORTED, "slices must be in 3..7");
   p->slices = S;
   size_t off = 0;
-  std::vector<SliceJob> jobs;
-  std::vector<int64_t> grp_begin;
+  std::vector<SliceTask> jobs;
   std::vector<GTile> tiles;
-  int64_t ngroups = 0;
   for (size_t bi = 0; bi < p->hblocks.size(); ++bi) {
     GBlock &b = p->hblocks[bi];
     const int64_t M = cplx ? 2 * b.m : b.m;
-    const int64_t K = cplx ? 2 * b.k : b.k;
     b.mpad = (int32_t)roundup(std::max<int64_t>(M, 1), PANEL_A);
     b.npad = (int32_t)roundup(std::max<int64_t>(b.n, 1), PANEL_B);
-    b.kpad = (int32_t)roundup(std::max<int64_t>(K, 1), KSTAGE);
+    // complex K: [Re | Im] halves of round_up(k, 16) positions each
+    b.kpad = cplx ? (int32_t)(2 * roundup(std::max<int64_t>(b.k, 1), 16))
+                  : (int32_t)roundup(std::max<int64_t>(b.k, 1), KSTAGE);
     if (b.m == 0 || b.n == 0 || b.skinny) continue;
     b.wsA = (int64_t)off;
     off += (size_t)S * b.mpad * b.kpad;
@@ -806,18 +1011,17 @@ int tkb_gemm_split_prepare(tkb_ctx *ctx, tkb_plan *p) {
     off = roundup((int64_t)off, 256);
     const int kind = b.k > 0 ? 0 : 1;
     if (kind == 0) {
-      const int64_t nkc = (b.kpad + KCHUNK - 1) / KCHUNK;  // K chunks (slicing tasks per row group)
-      jobs.push_back({(int32_t)bi, 0});
-      grp_begin.push_back(ngroups);
-      ngroups += (b.mpad / 32) * nkc;
-      jobs.push_back({(int32_t)bi, 1});
-      grp_begin.push_back(ngroups);
-      ngroups += (b.npad / 32) * nkc;
+      const int32_t kfull = cplx ? b.kpad / 2 : b.kpad;
+      const int32_t rows_a = cplx ? b.mpad / 2 : b.mpad;  // source rows (complex: row pairs)
+      for (int32_t r0 = 0; r0 < rows_a; r0 += 32) jobs.push_back({(int32_t)bi, 0, r0, kfull});
+      for (int32_t r0 = 0; r0 < b.npad; r0 += 32) jobs.push_back({(int32_t)bi, 1, r0, kfull});
     }
     for (int64_t m0 = 0; m0 < M; m0 += PANEL_A)
       for (int64_t n0 = 0; n0 < b.n; n0 += PANEL_B) tiles.push_back({(int32_t)bi, (int32_t)m0, (int32_t)n0, kind});
   }
-  // exponent arrays of every block in one contiguous region (reset to byte 0x80 per launch)
+  // slicing tasks: longest K first
+  std::stable_sort(jobs.begin(), jobs.end(), [](const SliceTask &x, const SliceTask &y) { return x.kfull > y.kfull; });
+  // exponent arrays of every block in one contiguous region (rewritten by every slicing pass)
   p->expo_off = (int64_t)off;
   for (size_t bi = 0; bi < p->hblocks.size(); ++bi) {
     GBlock &b = p->hblocks[bi];
@@ -832,19 +1036,37 @@ int tkb_gemm_split_prepare(tkb_ctx *ctx, tkb_plan *p) {
   std::stable_sort(tiles.begin(), tiles.end(), [&](const GTile &x, const GTile &y) {
     return p->hblocks[x.block].kpad > p->hblocks[y.block].kpad;
   });
-  // tcgen05 tasks: split the K range of tiles when there are too few tiles to occupy every
-  // SM twice, keeping at least two K stages per task
+  // tcgen05 tasks: one CTA per SM (the ring fills shared memory). With fewer tiles than SMs,
+  // the K loops are cut into pieces of about `target` stages, the smallest target (≥ 4
+  // stages) whose task count still fits one wave, so the longest task is as short as possible.
   std::vector<SplitTile> kt;
   int nslots = 0, npart = 0;
   {
     const int64_t nt = (int64_t)tiles.size();
-    int KS = 1;
-    // one CTA per SM (shared-memory ring): keep every task in the first wave
-    if (nt > 0 && nt < (int64_t)ctx->num_sms)
-      KS = (int)std::min<int64_t>(8, (int64_t)ctx->num_sms / nt);
+    const int64_t nsm = ctx->num_sms;
+    int64_t total = 0, maxnk = 1;
+    for (const GTile &t : tiles)
+      if (t.kind == 0) {
+        total += p->hblocks[t.block].kpad / KSTAGE;
+        maxnk = std::max<int64_t>(maxnk, p->hblocks[t.block].kpad / KSTAGE);
+      }
+    // int32 accumulators stay exact over at most (2^31 − 1)/(S·127²) K positions per task
+    const int64_t maxst = std::max<int64_t>(1, (int64_t)2147483647 / ((int64_t)S * 127 * 127) / KSTAGE);
+    auto pieces = [&](int64_t nk, int64_t target) {
+      return (int)std::max<int64_t>(std::min<int64_t>(8, (nk + target - 1) / target), (nk + maxst - 1) / maxst);
+    };
+    int64_t target = maxnk;  // no split
+    if (nt < nsm) {
+      target = std::max<int64_t>(4, (total + nsm - 1) / nsm);
+      for (; target < maxnk; ++target) {
+        int64_t cnt = 0;
+        for (const GTile &t : tiles) cnt += t.kind == 0 ? pieces(p->hblocks[t.block].kpad / KSTAGE, target) : 1;
+        if (cnt <= nsm) break;
+      }
+    }
     for (const GTile &t : tiles) {
       const int nk = p->hblocks[t.block].kpad / KSTAGE;
-      const int ks = t.kind == 0 ? std::max(1, std::min(KS, nk / 4)) : 1;  // ≥ 4 K stages per task
+      const int ks = t.kind == 0 ? pieces(nk, target) : 1;
       if (ks == 1) {
         kt.push_back({t.block, t.m0, t.n0, t.kind, 0, nk, -1, 1, 0, 0});
       } else {
@@ -862,7 +1084,7 @@ int tkb_gemm_split_prepare(tkb_ctx *ctx, tkb_plan *p) {
   p->nstiles = (int64_t)tiles.size();
   p->nkstiles = (int64_t)kt.size();
   p->nsjobs = (int)jobs.size();
-  p->nsrows = ngroups;
+  p->nsrows = (int64_t)jobs.size();
   cudaError_t e = cudaSuccess;
   if (!tiles.empty()) {
     e = cudaMalloc((void **)&p->stiles, tiles.size() * sizeof(GTile));
@@ -879,10 +1101,8 @@ int tkb_gemm_split_prepare(tkb_ctx *ctx, tkb_plan *p) {
     if (e == cudaSuccess) e = cudaMemset(p->pcnt, 0, nslots * sizeof(int));
   }
   if (e == cudaSuccess && !jobs.empty()) {
-    e = cudaMalloc(&p->sjobs, jobs.size() * sizeof(SliceJob));
-    if (e == cudaSuccess) e = cudaMemcpy(p->sjobs, jobs.data(), jobs.size() * sizeof(SliceJob), cudaMemcpyHostToDevice);
-    if (e == cudaSuccess) e = cudaMalloc((void **)&p->srow_begin, grp_begin.size() * 8);
-    if (e == cudaSuccess) e = cudaMemcpy(p->srow_begin, grp_begin.data(), grp_begin.size() * 8, cudaMemcpyHostToDevice);
+    e = cudaMalloc(&p->sjobs, jobs.size() * sizeof(SliceTask));
+    if (e == cudaSuccess) e = cudaMemcpy(p->sjobs, jobs.data(), jobs.size() * sizeof(SliceTask), cudaMemcpyHostToDevice);
   }
   if (e != cudaSuccess)
     return tkb_set_error(ctx, TKB_ERR_CUDA, std::string("split plan upload: ") + cudaGetErrorString(e));

@@ -82,7 +82,8 @@ struct GBlock {
   int32_t skinny;             // 1: n, k ≤ 16 — memory-bound row kernel in every precision
 };
 
-constexpr int kSkinnyMax = 16;  // n and k bound of the skinny (row-per-thread) path
+constexpr int kSkinnyMax = 16;        // n and k bound of the skinny (row-per-thread) path
+constexpr int kSkinnyMinRows = 2048;  // smaller blocks go to the tiled kernels
 constexpr int kSkinnyRows = 256;
 
 int tkb_gemm_skinny_launch(tkb_ctx *ctx, const tkb_plan *p, void *C, const void *A,
@@ -100,6 +101,7 @@ struct tkb_plan {
   int64_t nblocks = 0, ntiles = 0;
   GTile *sktasks = nullptr;     // skinny blocks: (block, first row) tasks of kSkinnyRows rows
   int64_t nsk = 0;
+  int sk_dim = 0;               // max(n, k) over the skinny blocks
   double flops = 0;
   int64_t lenA = 0, lenB = 0, lenC = 0;
   std::vector<GBlock> hblocks;
