@@ -57,6 +57,7 @@ struct tkb_table {
   int64_t ntasks = 0;
   int64_t elems_read = 0, elems_written = 0;
   int max_trees = 1;             // max(nsrc) over groups
+  bool single_tree = false;      // every group has one source and one destination tree
   size_t smem_f64 = 0;           // dynamic smem bytes needed for f64
   size_t smem_c128 = 0;
   int64_t src_len = 0, dst_len = 0;
@@ -65,6 +66,7 @@ struct tkb_table {
   int64_t *sstr = nullptr, *soff = nullptr, *dstr = nullptr, *doff = nullptr;
   double *coeffs = nullptr;
   int32_t *task_group = nullptr;  // ntasks: the group of every task
+  int32_t *task_idx = nullptr;    // ntasks × (2 + TKB_MAX_IND): tile coordinates, outer index
 };
 
 int tkb_transform_launch(tkb_ctx *ctx, const tkb_table *t, int dtype, void *dst,

@@ -17,6 +17,7 @@
 // All remaining dims are "outer": one task = one (tile_a, tile_b, outer index) of a group.
 // Tasks of all groups form one grid; groups arrive sorted by decreasing weight.
 #include <algorithm>
+#include <cstdlib>
 #include <cstring>
 #include <numeric>
 
@@ -28,6 +29,7 @@ constexpr int kThreads = 256;
 constexpr int kBatch = 8;  // elements per thread per load batch (loads in flight per thread)
 constexpr int64_t kTileElemsMax = 2048;  // largest task (= kThreads * kBatch elements)
 constexpr size_t kSmemBudget = 96 * 1024;
+constexpr int kTaskWords = 2 + TKB_MAX_IND;  // per task: tile a, tile b, outer multi-index
 
 struct CDbl {
   double x, y;
@@ -71,9 +73,10 @@ template <>
 __device__ __forceinline__ double2 scalar_from<double2>(CDbl s) { return make_double2(s.x, s.y); }
 
 template <typename T, bool CONJ>
-__global__ void __launch_bounds__(kThreads)
+__global__ void __launch_bounds__(kThreads, sizeof(T) == 8 ? 3 : 2)
     treetransform_kernel(const TGroup *__restrict__ groups, const int32_t *__restrict__ task_group,
-                         int ngroups, int64_t ntasks, const int64_t *__restrict__ sstr,
+                         const int32_t *__restrict__ task_idx, int64_t ntasks,
+                         const int64_t *__restrict__ sstr,
                          const int64_t *__restrict__ soff, const int64_t *__restrict__ dstr,
                          const int64_t *__restrict__ doff, const double *__restrict__ coeffs,
                          T *__restrict__ dst, const T *__restrict__ src, CDbl alpha_, CDbl beta_,
@@ -91,21 +94,12 @@ __global__ void __launch_bounds__(kThreads)
   const int64_t t_end = min(ntasks, t_begin + per);
   for (int64_t task = t_begin; task < t_end; ++task) {
     const TGroup &G = groups[task_group[task]];
-    int64_t t = task - G.task_begin;
-    const int64_t itb = t % G.ntile_b;
-    t /= G.ntile_b;
-    const int64_t ita = t % G.ntile_a;
-    int64_t o = t / G.ntile_a;
-    // outer multi-index -> per-tree base offsets computed lazily below
+    // tile coordinates and outer multi-index of the task, decomposed on the host
+    const int32_t *tix = task_idx + task * kTaskWords;
+    const int64_t ita = tix[0], itb = tix[1];
     int64_t oidx[TKB_MAX_IND];
 #pragma unroll
-    for (int q = 0; q < TKB_MAX_IND; ++q) {
-      if (q < G.nouter) {
-        const int64_t s = G.size[G.outer[q]];
-        oidx[q] = o % s;
-        o /= s;
-      }
-    }
+    for (int q = 0; q < TKB_MAX_IND; ++q) oidx[q] = q < G.nouter ? tix[2 + q] : 0;
     const int da = G.da, db = G.db;
     const int ta = G.ta, tb = G.tb;
     const int64_t a0 = ita * ta, b0 = itb * tb;
@@ -119,13 +113,17 @@ __global__ void __launch_bounds__(kThreads)
     auto src_base = [&](int64_t j) {
       const int64_t *st = sstr + (G.src_tree_begin + j) * TKB_MAX_IND;
       int64_t off = soff[G.src_tree_begin + j] + a0 * st[da] + (db >= 0 ? b0 * st[db] : 0);
-      for (int q = 0; q < G.nouter; ++q) off += oidx[q] * st[G.outer[q]];
+#pragma unroll
+      for (int q = 0; q < TKB_MAX_IND; ++q)
+        if (q < G.nouter) off += oidx[q] * st[G.outer[q]];
       return off;
     };
     auto dst_base = [&](int64_t i) {
       const int64_t *st = dstr + (G.dst_tree_begin + i) * TKB_MAX_IND;
       int64_t off = doff[G.dst_tree_begin + i] + a0 * st[da] + (db >= 0 ? b0 * st[db] : 0);
-      for (int q = 0; q < G.nouter; ++q) off += oidx[q] * st[G.outer[q]];
+#pragma unroll
+      for (int q = 0; q < TKB_MAX_IND; ++q)
+        if (q < G.nouter) off += oidx[q] * st[G.outer[q]];
       return off;
     };
 
@@ -220,6 +218,155 @@ __global__ void __launch_bounds__(kThreads)
   }
 }
 
+// ---- pipelined kernel for tables of single-tree groups (nsrc = ndst = 1) -----------------
+// Abelian transformers and fusion blocks with one tree pair are pure strided copies with one
+// coefficient. A persistent CTA walks its contiguous range of tasks with a kPipeStages-deep
+// ring of shared-memory tiles: the source tile of task i + kPipeStages is requested with
+// cp.async while task i is written out, so the read stream never waits for the writes.
+// Tiles are staged in the layout the writes want (transpose mode: pitch tb + 1).
+constexpr int kPipeStages = 3;
+constexpr int kStageElems = kTileElemsMax + 256;
+
+struct TaskGeo {
+  int64_t sbase, dbase, sA, sB, dA, dB;
+  int na, nb, ta, lta, ltb, tot, mode, pitch;
+  double u;
+};
+
+__device__ __forceinline__ TaskGeo task_geo(int64_t task, const TGroup *__restrict__ groups,
+                                            const int32_t *__restrict__ task_group,
+                                            const int32_t *__restrict__ task_idx,
+                                            const int64_t *__restrict__ sstr, const int64_t *__restrict__ soff,
+                                            const int64_t *__restrict__ dstr, const int64_t *__restrict__ doff,
+                                            const double *__restrict__ coeffs) {
+  const TGroup &G = groups[task_group[task]];
+  const int32_t *tix = task_idx + task * kTaskWords;
+  const int da = G.da, db = G.db;
+  const int64_t a0 = (int64_t)tix[0] * G.ta, b0 = (int64_t)tix[1] * G.tb;
+  const int64_t *ss = sstr + G.src_tree_begin * TKB_MAX_IND;
+  const int64_t *ds = dstr + G.dst_tree_begin * TKB_MAX_IND;
+  TaskGeo g;
+  g.sA = ss[da];
+  g.dA = ds[da];
+  g.sB = db >= 0 ? ss[db] : 0;
+  g.dB = db >= 0 ? ds[db] : 0;
+  int64_t so = soff[G.src_tree_begin] + a0 * g.sA + b0 * g.sB;
+  int64_t dof = doff[G.dst_tree_begin] + a0 * g.dA + b0 * g.dB;
+#pragma unroll
+  for (int q = 0; q < TKB_MAX_IND; ++q)
+    if (q < G.nouter) {
+      const int64_t o = tix[2 + q];
+      so += o * ss[G.outer[q]];
+      dof += o * ds[G.outer[q]];
+    }
+  g.sbase = so;
+  g.dbase = dof;
+  const int64_t sa = G.size[da], sb = db >= 0 ? G.size[db] : 1;
+  g.na = (int)(sa - a0 < G.ta ? sa - a0 : G.ta);
+  g.nb = (int)(sb - b0 < G.tb ? sb - b0 : G.tb);
+  g.ta = G.ta;
+  g.lta = __ffs(G.ta) - 1;
+  g.ltb = __ffs(G.tb) - 1;
+  g.tot = G.ta * G.tb;
+  g.mode = G.mode;
+  g.pitch = G.tb + 1;
+  g.u = coeffs[G.coeff_begin];
+  return g;
+}
+
+__device__ __forceinline__ void cp_async_el(double *sm, const double *g) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"((unsigned)__cvta_generic_to_shared(sm)),
+               "l"(g)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async_el(double2 *sm, const double2 *g) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"((unsigned)__cvta_generic_to_shared(sm)),
+               "l"(g)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+__device__ __forceinline__ double conj_v(double v, bool) { return v; }
+__device__ __forceinline__ double2 conj_v(double2 v, bool c) {
+  if (c) v.y = -v.y;
+  return v;
+}
+
+template <typename T, bool CONJ>
+__global__ void __launch_bounds__(kThreads)
+    treetransform_pipe_kernel(const TGroup *__restrict__ groups, const int32_t *__restrict__ task_group,
+                              const int32_t *__restrict__ task_idx, int64_t ntasks,
+                              const int64_t *__restrict__ sstr, const int64_t *__restrict__ soff,
+                              const int64_t *__restrict__ dstr, const int64_t *__restrict__ doff,
+                              const double *__restrict__ coeffs, T *__restrict__ dst,
+                              const T *__restrict__ src, CDbl alpha_, CDbl beta_, int beta_zero) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T *sm = reinterpret_cast<T *>(smem_raw);
+  const T alpha = scalar_from<T>(alpha_);
+  const T beta = scalar_from<T>(beta_);
+  const bool bz = beta_zero != 0;
+  const int64_t per = (ntasks + gridDim.x - 1) / gridDim.x;
+  const int64_t t_begin = (int64_t)blockIdx.x * per;
+  const int64_t t_end = min(ntasks, t_begin + per);
+
+  auto issue = [&](int64_t task, T *stage) {
+    const TaskGeo g = task_geo(task, groups, task_group, task_idx, sstr, soff, dstr, doff, coeffs);
+    for (int e = threadIdx.x; e < g.tot; e += kThreads) {
+      int ia, ib, si;
+      if (g.mode == 1) {  // source-fast b: coalesced reads, tile stored row-pitched
+        ia = e >> g.ltb;
+        ib = e & ((1 << g.ltb) - 1);
+        si = ia * g.pitch + ib;
+      } else {
+        ia = e & (g.ta - 1);
+        ib = e >> g.lta;
+        si = ib * g.ta + ia;
+      }
+      if (ia < g.na && ib < g.nb) cp_async_el(stage + si, src + g.sbase + ia * g.sA + ib * g.sB);
+    }
+  };
+  auto write = [&](int64_t task, const T *stage) {
+    const TaskGeo g = task_geo(task, groups, task_group, task_idx, sstr, soff, dstr, doff, coeffs);
+    for (int e0 = 0; e0 < g.tot; e0 += kThreads * kBatch) {
+#pragma unroll
+      for (int q = 0; q < kBatch; ++q) {
+        const int e = e0 + q * kThreads + threadIdx.x;
+        const int ia = e & (g.ta - 1), ib = e >> g.lta;  // a fastest: coalesced writes
+        if (e < g.tot && ia < g.na && ib < g.nb) {
+          const T v = conj_v(stage[g.mode == 1 ? ia * g.pitch + ib : ib * g.ta + ia], CONJ);
+          T *dp = dst + g.dbase + ia * g.dA + ib * g.dB;
+          *dp = finish(axpy_r(g.u, v, zero_val(T{})), alpha, beta, dp, bz);
+        }
+      }
+    }
+  };
+#pragma unroll
+  for (int st = 0; st < kPipeStages; ++st) {
+    if (t_begin + st < t_end) issue(t_begin + st, sm + st * kStageElems);
+    cp_async_commit();
+  }
+  int st = 0;
+  for (int64_t task = t_begin; task < t_end; ++task) {
+    cp_async_wait<kPipeStages - 1>();
+    __syncthreads();
+    write(task, sm + st * kStageElems);
+    __syncthreads();
+    if (task + kPipeStages < t_end) issue(task + kPipeStages, sm + st * kStageElems);
+    cp_async_commit();
+    st = st + 1 == kPipeStages ? 0 : st + 1;
+  }
+  cp_async_wait<0>();
+}
+
+// TKB_TRANSFORM_KERNEL=plain selects the non-pipelined kernel for every table (comparison)
+bool use_plain_transform() {
+  const char *e = std::getenv("TKB_TRANSFORM_KERNEL");
+  return e && std::strcmp(e, "plain") == 0;
+}
+
 int64_t pow2ceil(int64_t x) {
   int64_t p = 1;
   while (p < x) p <<= 1;
@@ -251,10 +398,11 @@ extern "C" int tkb_table_create(tkb_ctx *ctx, const tkb_table_desc *d, tkb_table
   hg.reserve(G);
   std::vector<int64_t> hsstr, hsoff, hdstr, hdoff;
   std::vector<int32_t> htask;  // task → group
+  std::vector<int32_t> hidx;   // task → (tile a, tile b, outer multi-index)
   std::vector<double> hcoef;
   int64_t ntasks = 0, er = 0, ew = 0;
   size_t smem_max_f64 = 0, smem_max_c128 = 0;
-  int max_trees = 1;
+  int max_trees = 1, max_dst = 1;
   // tile target: 2048 elements per task, smaller when the whole transform would not give
   // every SM about four tasks (small permutes are latency-bound, not bandwidth-bound)
   int64_t kTileElems = kTileElemsMax;
@@ -348,7 +496,11 @@ extern "C" int tkb_table_create(tkb_ctx *ctx, const tkb_table_desc *d, tkb_table
     TGroup tg;
     std::memset(&tg, 0, sizeof(tg));
     tg.ndim = nd;
-    for (int k = 0; k < nd; ++k) tg.size[k] = dims[k].size;
+    for (int k = 0; k < nd; ++k) {
+      if (dims[k].size > INT32_MAX)
+        return tkb_set_error(ctx, TKB_ERR_UNSUPPORTED, "sub-block dimension beyond 2^31 elements");
+      tg.size[k] = dims[k].size;
+    }
     // fastest dims (tree 0 pattern; all trees of a group share it)
     int fa = 0, fs = 0;
     for (int k = 1; k < nd; ++k) {
@@ -422,7 +574,22 @@ extern "C" int tkb_table_create(tkb_ctx *ctx, const tkb_table_desc *d, tkb_table
       smem_max_c128 = std::max(smem_max_c128, (size_t)(nsrc * te) * el128);
     }
     max_trees = std::max<int>(max_trees, (int)nsrc);
+    max_dst = std::max<int>(max_dst, (int)ndst);
     htask.insert(htask.end(), (size_t)(ntasks - tg.task_begin), (int32_t)g);
+    for (int64_t t = 0; t < ntasks - tg.task_begin; ++t) {
+      int64_t r = t;
+      int32_t w[kTaskWords] = {0};
+      w[1] = (int32_t)(r % tg.ntile_b);
+      r /= tg.ntile_b;
+      w[0] = (int32_t)(r % tg.ntile_a);
+      r /= tg.ntile_a;
+      for (int q = 0; q < tg.nouter; ++q) {
+        const int64_t sq = tg.size[tg.outer[q]];
+        w[2 + q] = (int32_t)(r % sq);
+        r /= sq;
+      }
+      hidx.insert(hidx.end(), w, w + kTaskWords);
+    }
     hg.push_back(tg);
   }
   if (std::max(smem_max_f64, smem_max_c128) > ctx->smem_optin)
@@ -435,6 +602,7 @@ extern "C" int tkb_table_create(tkb_ctx *ctx, const tkb_table_desc *d, tkb_table
   t->elems_read = er;
   t->elems_written = ew;
   t->max_trees = max_trees;
+  t->single_tree = max_trees == 1 && max_dst == 1;
   t->smem_f64 = smem_max_f64;
   t->smem_c128 = smem_max_c128;
   t->src_len = d->src_len;
@@ -448,6 +616,7 @@ extern "C" int tkb_table_create(tkb_ctx *ctx, const tkb_table_desc *d, tkb_table
   cudaError_t e = cudaSetDevice(ctx->device);
   if (e == cudaSuccess) e = up((void **)&t->groups, hg.data(), hg.size() * sizeof(TGroup));
   if (e == cudaSuccess) e = up((void **)&t->task_group, htask.data(), htask.size() * 4);
+  if (e == cudaSuccess) e = up((void **)&t->task_idx, hidx.data(), hidx.size() * 4);
   if (e == cudaSuccess) e = up((void **)&t->sstr, hsstr.data(), hsstr.size() * 8);
   if (e == cudaSuccess) e = up((void **)&t->soff, hsoff.data(), hsoff.size() * 8);
   if (e == cudaSuccess) e = up((void **)&t->dstr, hdstr.data(), hdstr.size() * 8);
@@ -466,6 +635,7 @@ extern "C" int tkb_table_destroy(tkb_table *t) {
   if (!t) return TKB_OK;
   cudaFree(t->groups);
   cudaFree(t->task_group);
+  cudaFree(t->task_idx);
   cudaFree(t->sstr);
   cudaFree(t->soff);
   cudaFree(t->dstr);
@@ -489,20 +659,44 @@ int tkb_transform_launch(tkb_ctx *ctx, const tkb_table *t, int dtype, void *dst,
   const int grid = (int)std::min<int64_t>(t->ntasks, (int64_t)ctx->num_sms * 16);
   CDbl a{alpha.re, alpha.im}, b{beta.re, beta.im};
   const int bz = (beta.re == 0.0 && beta.im == 0.0) ? 1 : 0;
+  if (t->single_tree && (dtype == TKB_F64 || dtype == TKB_C128) && !use_plain_transform()) {
+    if (dtype == TKB_F64 && (alpha.im != 0.0 || beta.im != 0.0))
+      return tkb_set_error(ctx, TKB_ERR_ARG, "complex scalar with real data");
+    // persistent CTAs, as many as the stage ring lets reside (4 real / 2 complex per SM)
+    const size_t el = dtype == TKB_F64 ? 8 : 16;
+    const size_t smem = (size_t)kPipeStages * kStageElems * el;
+    const int pgrid = (int)std::min<int64_t>(t->ntasks, (int64_t)ctx->num_sms * (dtype == TKB_F64 ? 4 : 2));
+    if (dtype == TKB_F64) {
+      auto k = treetransform_pipe_kernel<double, false>;
+      TKB_CUDA_TRY(ctx, cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+      k<<<pgrid, kThreads, smem, ctx->stream>>>(t->groups, t->task_group, t->task_idx, t->ntasks, t->sstr,
+                                               t->soff, t->dstr, t->doff, t->coeffs, (double *)dst,
+                                               (const double *)src, a, b, bz);
+    } else {
+      auto k = conj ? treetransform_pipe_kernel<double2, true> : treetransform_pipe_kernel<double2, false>;
+      TKB_CUDA_TRY(ctx, cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+      k<<<pgrid, kThreads, smem, ctx->stream>>>(t->groups, t->task_group, t->task_idx, t->ntasks, t->sstr,
+                                               t->soff, t->dstr, t->doff, t->coeffs, (double2 *)dst,
+                                               (const double2 *)src, a, b, bz);
+    }
+    ctx->launches++;
+    TKB_CUDA_TRY(ctx, cudaGetLastError());
+    return TKB_OK;
+  }
   if (dtype == TKB_F64) {
     if (alpha.im != 0.0 || beta.im != 0.0)
       return tkb_set_error(ctx, TKB_ERR_ARG, "complex scalar with real data");
     const size_t smem = t->smem_f64;
     auto k = treetransform_kernel<double, false>;
     if (smem > 48 * 1024) TKB_CUDA_TRY(ctx, cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    k<<<grid, kThreads, smem, ctx->stream>>>(t->groups, t->task_group, t->ngroups, t->ntasks,
+    k<<<grid, kThreads, smem, ctx->stream>>>(t->groups, t->task_group, t->task_idx, t->ntasks,
                                             t->sstr, t->soff, t->dstr, t->doff, t->coeffs,
                                             (double *)dst, (const double *)src, a, b, bz);
   } else if (dtype == TKB_C128) {
     const size_t smem = t->smem_c128;
     auto k = conj ? treetransform_kernel<double2, true> : treetransform_kernel<double2, false>;
     if (smem > 48 * 1024) TKB_CUDA_TRY(ctx, cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    k<<<grid, kThreads, smem, ctx->stream>>>(t->groups, t->task_group, t->ngroups, t->ntasks,
+    k<<<grid, kThreads, smem, ctx->stream>>>(t->groups, t->task_group, t->task_idx, t->ntasks,
                                             t->sstr, t->soff, t->dstr, t->doff, t->coeffs,
                                             (double2 *)dst, (const double2 *)src, a, b, bz);
   } else {
