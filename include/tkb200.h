@@ -102,6 +102,39 @@ int tkb_table_info(const tkb_table *table, int64_t *ntasks, int64_t *elems_read,
 int tkb_treetransform(tkb_ctx *ctx, const tkb_table *table, int dtype, void *dst,
                       const void *src, tkb_scalar alpha, tkb_scalar beta, int conj_src);
 
+/* ---- partial-trace tables ------------------------------------------------------------ */
+/* Flattened trace_permute! (src/tensors/tensoroperations.jl:212-296): one group per
+ * destination sub-block (every sub-block of the destination, so that β reaches all of
+ * them); its entries are the source sub-blocks whose permuted trees split into it, with the
+ * recoupling coefficient times dim(g.coupled)/dim(g.uncoupled[1]).
+ *   dst_g[x] = β·dst_g[x] + α·Σ_e coeff_e · Σ_t src[off_e + Σ_k x_k·str_e,k + Σ_l t_l·tstr_e,l]
+ * x runs over the group's free sizes (destination order), t over the entry's traced sizes,
+ * tstr_e,l = stride(q₁[l]) + stride(q₂[l]) of the source sub-block. */
+typedef struct tkb_trace_desc {
+  int32_t nfree;                 /* free legs, ≤ TKB_MAX_IND */
+  int32_t ntrace;                /* traced leg pairs, 1..TKB_MAX_IND */
+  int64_t ngroups;
+  const int64_t *group_entry_ptr;  /* ngroups+1: prefix sums of entries per group */
+  const int64_t *sizes;            /* ngroups*nfree: free sizes */
+  const int64_t *dst_strides;      /* ngroups*nfree */
+  const int64_t *dst_offsets;      /* ngroups */
+  const int64_t *src_strides;      /* nentries*nfree: source strides of the free legs */
+  const int64_t *trace_sizes;      /* nentries*ntrace */
+  const int64_t *trace_strides;    /* nentries*ntrace */
+  const int64_t *src_offsets;      /* nentries */
+  const double *coeffs;            /* nentries */
+  int64_t src_len, dst_len;        /* elements in the data vectors (bounds check) */
+} tkb_trace_desc;
+
+typedef struct tkb_trace_table tkb_trace_table;
+/* replaces the per-sub-block TO.tensortrace! calls of _trace_permute!
+ * (src/tensors/tensoroperations.jl:246-296) with one table built once per structure */
+int tkb_trace_table_create(tkb_ctx *ctx, const tkb_trace_desc *desc, tkb_trace_table **out);
+int tkb_trace_table_destroy(tkb_trace_table *table);
+/* conj_src != 0 reads the source with complex conjugation (lazy adjoint source) */
+int tkb_tracetransform(tkb_ctx *ctx, const tkb_trace_table *table, int dtype, void *dst,
+                       const void *src, tkb_scalar alpha, tkb_scalar beta, int conj_src);
+
 /* ---- grouped block GEMM ------------------------------------------------------------- */
 /* C_b = α·op(A_b)·op(B_b) + β·C_b for every block b; column-major blocks in flat vectors.
  * op(A_b) is m×k, op(B_b) is k×n. Blocks with k = 0 scale C_b by β. */

@@ -27,6 +27,7 @@ Reference citations (TensorKit.jl v0.17.1):
   add_transform    src/tensors/indexmanipulations.jl:658-726
   mul/norm/tr      src/tensors/linalg.jl:257-282,319-370; inner src/tensors/vectorinterface.jl:114-130
   contract         src/tensors/tensoroperations.jl:130-161,318-462
+  trace            src/tensors/tensoroperations.jl:212-296, src/fusiontrees/basic_manipulations.jl:30-52
 """
 from __future__ import annotations
 
@@ -592,6 +593,61 @@ def permute(t: BT, p, alpha=1.0, adjoint=False, tdst=None, beta=0.0):
                 continue
             d = res.sub(dpair)
             d += (alpha * x) * moved
+    return res
+
+
+def split_tree(f, M):
+    """(f₁, f₂): f₁ keeps the first M uncoupled legs and couples to the line between them and
+    the rest; f₂ starts with that line (src/fusiontrees/basic_manipulations.jl:30-52)."""
+    u, c, d, inner = f
+    N = len(u)
+    ext = (u[0],) + tuple(inner) + (c,) if N > 0 else (c,)
+    c1 = unit(c) if M == 0 else ext[M - 1]
+    f1 = (u[:M], c1, d[:M], tuple(inner[:max(0, M - 2)]))
+    f2 = ((c1,) + u[M:], c, (False,) + d[M:], tuple(ext[M:M + max(0, N - M - 1)]))
+    return f1, f2
+
+
+def trace_permute(t: BT, p, q, alpha=1.0, tdst=None, beta=0.0):
+    """β·tdst + α·(permute t by p, tracing the leg pairs q = (q₁, q₂)) for bosonic sectors
+    (src/tensors/tensoroperations.jl:212-296): every tree pair is permuted to
+    ((p₁, q₁), (p₂, q₂)); both trees are split after the kept legs, pairs whose split-off
+    trees differ vanish, the others carry dim(g.coupled)/dim(g.uncoupled[1]) and a dense
+    partial trace of the sub-block."""
+    W = t.W
+    p1, p2 = tuple(p[0]), tuple(p[1])
+    q1, q2 = tuple(q[0]), tuple(q[1])
+    N1, N2 = len(p1), len(p2)
+    Wdst = W.select((p1, p2))
+    total = layout(Wdst)[0]
+    out = np.zeros(total, dtype=t.data.dtype) if tdst is None else tdst.data * beta
+    res = BT(Wdst, out)
+    r = (p1 + q1, p2 + q2)
+    letters = "abcdefghijklmnopqrstuvwxyzABCDEFGHIJKLMNOPQRSTUVWXYZ"
+    nlegs = W.n1() + W.n2()
+    sub_in = [""] * nlegs
+    k = 0
+    for x in p1 + p2:
+        sub_in[x - 1] = letters[k]
+        k += 1
+    for a, b in zip(q1, q2):
+        sub_in[a - 1] = sub_in[b - 1] = letters[k]
+        k += 1
+    spec = "".join(sub_in) + "->" + "".join(sub_in[x - 1] for x in p1 + p2)
+    for pair in layout(W)[3]:
+        src = t.sub(pair)
+        traced = None
+        for (f1p, f2p), x in permute_pair(pair, r).items():
+            if x == 0.0:
+                continue
+            h1, g1 = split_tree(f1p, N1)
+            h2, g2 = split_tree(f2p, N2)
+            if g1 != g2:
+                continue
+            x = x * qdim(g1[1]) / qdim(g1[0][0])
+            if traced is None:
+                traced = np.einsum(spec, src)
+            res.sub((h1, h2))[...] += (alpha * x) * traced
     return res
 
 

@@ -72,6 +72,35 @@ struct tkb_table {
 int tkb_transform_launch(tkb_ctx *ctx, const tkb_table *t, int dtype, void *dst,
                          const void *src, tkb_scalar alpha, tkb_scalar beta, int conj);
 
+// partial trace --------------------------------------------------------------------------
+struct TrGroup {
+  int64_t dst_off;
+  int64_t e_begin, e_end;   // entries of this destination sub-block
+  int64_t nelem;            // product of the free sizes
+  int64_t task_begin;
+  int32_t size[TKB_MAX_IND];
+  int64_t dstr[TKB_MAX_IND];
+};
+
+struct TrEntry {
+  int64_t src_off;
+  double coeff;
+  int64_t ntr_total;        // product of the traced sizes
+  int64_t sstr[TKB_MAX_IND];
+  int32_t tsize[TKB_MAX_IND];
+  int64_t tstr[TKB_MAX_IND];
+};
+
+struct tkb_trace_table {
+  tkb_ctx *owner = nullptr;
+  int nfree = 0, ntrace = 0;
+  int64_t ngroups = 0, ntasks = 0;
+  int64_t src_len = 0, dst_len = 0;
+  TrGroup *groups = nullptr;
+  TrEntry *entries = nullptr;
+  int32_t *task_group = nullptr;
+};
+
 // grouped gemm --------------------------------------------------------------------------
 struct GBlock {
   int64_t m, n, k;

@@ -19,7 +19,9 @@ from .indexmanipulations import (permute, permute_, braid, braid_, transpose, tr
                                  repartition, add_transform_)
 from .linalg import mul_, compose, norm, tr, inner, dot, scale_, add_
 from .tensoroperations import (tensoradd_, tensorcontract_, tensorcontract, contract_,
-                               tensor, tensorcontract_structure, tensoradd_structure)
+                               tensor, tensorcontract_structure, tensoradd_structure,
+                               tensortrace_, tensortrace, tensortrace_structure)
+from .trace import trace_permute_, trace_permute
 from .network import NetworkPlan
 
 __version__ = "0.1.0"

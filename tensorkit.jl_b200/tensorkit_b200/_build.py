@@ -8,7 +8,7 @@ import sys
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 CSRC = os.path.join(ROOT, "csrc")
 LIBDIR = os.path.join(ROOT, "lib")
-SOURCES = ["capi.cu", "transform.cu", "gemm_f64.cu", "gemm_split.cu", "reduce.cu"]
+SOURCES = ["capi.cu", "transform.cu", "trace.cu", "gemm_f64.cu", "gemm_split.cu", "reduce.cu"]
 NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "-std=c++17",
               "-Xcompiler", "-fPIC", "-shared"]
 

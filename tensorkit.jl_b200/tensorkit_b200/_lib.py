@@ -25,7 +25,8 @@ TKB_NORM2, TKB_INNER, TKB_TRACE = 0, 1, 2
 EXPORTS = [
     "tkb_version", "tkb_ctx_create", "tkb_ctx_destroy", "tkb_ctx_set_stream",
     "tkb_ctx_synchronize", "tkb_ctx_launch_count", "tkb_last_error", "tkb_table_create",
-    "tkb_table_destroy", "tkb_table_info", "tkb_treetransform", "tkb_gemm_plan_create",
+    "tkb_table_destroy", "tkb_table_info", "tkb_treetransform", "tkb_trace_table_create",
+    "tkb_trace_table_destroy", "tkb_tracetransform", "tkb_gemm_plan_create",
     "tkb_gemm_plan_destroy", "tkb_gemm_plan_info", "tkb_grouped_gemm", "tkb_rplan_create",
     "tkb_rplan_destroy", "tkb_reduce", "tkb_reduce_async", "tkb_reduce_noalloc",
     "tkb_graph_begin", "tkb_graph_end",
@@ -43,6 +44,16 @@ class tkb_table_desc(C.Structure):
         ("group_src_ptr", C.c_void_p), ("group_dst_ptr", C.c_void_p), ("coeff_ptr", C.c_void_p),
         ("coeffs", C.c_void_p), ("sizes", C.c_void_p), ("src_strides", C.c_void_p),
         ("src_offsets", C.c_void_p), ("dst_strides", C.c_void_p), ("dst_offsets", C.c_void_p),
+        ("src_len", C.c_int64), ("dst_len", C.c_int64),
+    ]
+
+
+class tkb_trace_desc(C.Structure):
+    _fields_ = [
+        ("nfree", C.c_int32), ("ntrace", C.c_int32), ("ngroups", C.c_int64),
+        ("group_entry_ptr", C.c_void_p), ("sizes", C.c_void_p), ("dst_strides", C.c_void_p),
+        ("dst_offsets", C.c_void_p), ("src_strides", C.c_void_p), ("trace_sizes", C.c_void_p),
+        ("trace_strides", C.c_void_p), ("src_offsets", C.c_void_p), ("coeffs", C.c_void_p),
         ("src_len", C.c_int64), ("dst_len", C.c_int64),
     ]
 
@@ -83,6 +94,9 @@ def _declare(lib):
         "tkb_table_destroy": ([vp], C.c_int),
         "tkb_table_info": ([vp, P(i64), P(i64), P(i64)], C.c_int),
         "tkb_treetransform": ([vp, vp, C.c_int, vp, vp, tkb_scalar, tkb_scalar, C.c_int], C.c_int),
+        "tkb_trace_table_create": ([vp, P(tkb_trace_desc), P(vp)], C.c_int),
+        "tkb_trace_table_destroy": ([vp], C.c_int),
+        "tkb_tracetransform": ([vp, vp, C.c_int, vp, vp, tkb_scalar, tkb_scalar, C.c_int], C.c_int),
         "tkb_gemm_plan_create": ([vp, P(tkb_gemm_desc), P(vp)], C.c_int),
         "tkb_gemm_plan_destroy": ([vp], C.c_int),
         "tkb_gemm_plan_info": ([vp, P(dbl), P(i32)], C.c_int),

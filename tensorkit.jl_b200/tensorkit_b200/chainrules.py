@@ -9,6 +9,8 @@ Restates `ext/TensorKitChainRulesCoreExt/tensoroperations.jl` and `src/pullbacks
   ipA = repartition(invperm(linearize(pA)), numout(A)) (and likewise ipB). Twists are
   trivial for bosonic sectors.
 - `rrule_tensoradd` (`:8-58`): dA = tensoradd(ΔC, pdA, conjA, conjA ? α : conj(α)).
+- `rrule_tensortrace` (`:152-199`): dA = ΔC ⊗ id(traced legs), permuted back, times
+  conj(α) (α when conjA).
 - `rrule_permute` (`src/pullbacks/indexmanipulations.jl:1-31`, `ext/.../linalg.jl:62-70`):
   the inverse permutation with conj(α).
 - `rrule_tr`: Δ ↦ conj(Δ)·id;  `rrule_norm`: Δ ↦ (Δ/‖t‖)·t.
@@ -31,7 +33,8 @@ from .tensoroperations import (_alloc, _pairwise_steps, parse_tensor_expr, tenso
                                tensoradd_structure, tensorcontract, tensorcontract_,
                                tensorcontract_structure)
 
-__all__ = ["rrule_tensorcontract", "rrule_tensoradd", "rrule_permute", "rrule_tr", "rrule_norm",
+__all__ = ["rrule_tensorcontract", "rrule_tensoradd", "rrule_tensortrace", "rrule_permute", "rrule_tr",
+           "rrule_norm",
            "network_with_pullback", "TensorContract"]
 
 
@@ -106,6 +109,48 @@ def rrule_tensoradd(C, A, pA, conjA, alpha=1.0, beta=0.0):
             from .linalg import scale_
             scale_(dC, _conj(beta))
         return dC, dA
+
+    return Cp, pullback
+
+
+def _identity(W, like):
+    """one!(TensorMap of space W): identity blocks (W must be square)."""
+    import torch
+    from .structure import blockstructure
+    out = TensorMap(torch.zeros(W.dim(), dtype=like.data.dtype, device=like.data.device), W)
+    for c, ((d1, d2), (a, _)) in blockstructure(W).items():
+        out.data[a:a + d1 * d2].view(d2, d1).diagonal().fill_(1.0)
+    return out
+
+
+def rrule_tensortrace(C, A, p, q, conjA=False, alpha=1.0, beta=0.0):
+    """Returns (C′, pullback) with C′ = β·C + α·tensortrace(op(A), p, q); pullback(ΔC) →
+    (dC, dA, dα, dβ) following `ext/TensorKitChainRulesCoreExt/tensoroperations.jl:152-199`:
+    dA = tensorproduct(ΔC, (trivial(p); ()), conjA, E, ((); trivial(q)), conjA, pdA,
+    conjA ? α : conj(α)) with E = one!(space of the traced legs) and
+    pdA = repartition(invperm((linearize(p)..., q₁..., q₂...)), numout(A)); twists are
+    trivial for bosonic sectors."""
+    from .tensoroperations import tensortrace, tensortrace_
+    Cp = TensorMap(C.data.clone(), C.space)
+    tensortrace_(Cp, A, p, q, conjA, alpha, beta)
+
+    def pullback(dC_):
+        dC = None
+        if beta != 0:
+            dC = TensorMap(dC_.data.clone(), dC_.space)
+            from .linalg import scale_
+            scale_(dC, _conj(beta))
+        ip = _invperm(_lin(p) + tuple(q[0]) + tuple(q[1]))
+        pdA = _rep(ip, A.numout())
+        E = _identity(tensoradd_structure(A, q, conjA), A)
+        nq = len(q[0]) + len(q[1])
+        np_ = len(p[0]) + len(p[1])
+        pE = ((), tuple(range(1, nq + 1)))
+        pdC = (tuple(range(1, np_ + 1)), ())
+        dA = tensorcontract(dC_, pdC, conjA, E, pE, conjA, pdA, alpha if conjA else _conj(alpha))
+        dalpha = inner(tensortrace(A, p, q, conjA), dC_)
+        dbeta = inner(C, dC_)
+        return dC, dA, dalpha, dbeta
 
     return Cp, pullback
 

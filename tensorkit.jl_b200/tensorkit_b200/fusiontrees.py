@@ -22,7 +22,7 @@ import numpy as np
 from .sectors import (Bsymbol, Fsymbol, Nsymbol, Rsymbol, frobenius_schur_phase,
                       invsqrtdim, otimes_many, sqrtdim)
 
-__all__ = ["FusionTree", "FusionTreeBlock", "fusiontrees", "bendright", "bendleft",
+__all__ = ["FusionTree", "FusionTreeBlock", "fusiontrees", "bendright", "bendleft", "split",
            "repartition", "artin_braid", "braid", "permute", "linearizepermutation",
            "permutation2swaps"]
 
@@ -216,6 +216,21 @@ def bendleft(src):
         (a, b, c), (f2n, f1n) = _bendright_treepair(f2, f1)
         U[dst.index[(f1n, f2n)], col] = _bend_coeff(a, b, c, f2.isdual[-1])
     return dst, U
+
+
+def split(f, M):
+    """(f₁, f₂) with f₁ the first M uncoupled legs of f fused to the line c₁ between them and
+    the rest, and f₂ = (c₁, remaining legs) → f.coupled
+    (`src/fusiontrees/basic_manipulations.jl:30-52`)."""
+    N = len(f.uncoupled)
+    if not 0 <= M <= N or N == 0:
+        raise ValueError("split: M must lie in 0..N (N ≥ 1)")
+    ext = (f.uncoupled[0],) + tuple(f.innerlines) + (f.coupled,)
+    c1 = f.coupled.unit() if M == 0 else ext[M - 1]
+    f1 = FusionTree(f.uncoupled[:M], c1, f.isdual[:M], f.innerlines[:max(0, M - 2)])
+    f2 = FusionTree((c1,) + f.uncoupled[M:], f.coupled, (False,) + f.isdual[M:],
+                    ext[M:M + max(0, N - M - 1)])
+    return f1, f2
 
 
 def repartition(src, N):

@@ -36,11 +36,11 @@ LAUNCH_LOG: list | None = None
 def relaunch(entry):
     """Re-issue one recorded launch with the same operands (for kernel timing)."""
     ctx = entry[1].ctx
-    if entry[0] == "transform":
+    if entry[0] in ("transform", "trace"):
         _, table, tdst, tsrc, a, b, conj = entry
-        L.check(ctx.lib.tkb_treetransform(ctx.handle, table.handle, dtype_code(tdst.data),
-                                          C.c_void_p(tdst.data.data_ptr()), C.c_void_p(tsrc.data.data_ptr()),
-                                          _scalar(a), _scalar(b), conj), ctx.handle)
+        fn = ctx.lib.tkb_treetransform if entry[0] == "transform" else ctx.lib.tkb_tracetransform
+        L.check(fn(ctx.handle, table.handle, dtype_code(tdst.data), C.c_void_p(tdst.data.data_ptr()),
+                   C.c_void_p(tsrc.data.data_ptr()), _scalar(a), _scalar(b), conj), ctx.handle)
     else:
         _, plan, tC, tA, tB, a, b = entry
         L.check(ctx.lib.tkb_grouped_gemm(ctx.handle, plan.handle, C.c_void_p(tC.data.data_ptr()),

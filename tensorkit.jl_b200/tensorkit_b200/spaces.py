@@ -123,7 +123,9 @@ class ProductSpace:
                 raise ValueError("empty ProductSpace needs an explicit unit sector")
             unit = self.spaces[0].unit()
         self._unit = unit
-        self._h = hash(("PS",) + self.spaces)
+        # the unit sector is part of the identity: spaces without legs of different sector
+        # types (one(Vect[U1Irrep]) vs one(Vect[SU2Irrep])) must not compare equal
+        self._h = hash(("PS", unit) + self.spaces)
 
     def __len__(self):
         return len(self.spaces)
@@ -135,7 +137,7 @@ class ProductSpace:
         return iter(self.spaces)
 
     def __eq__(self, o):
-        return isinstance(o, ProductSpace) and o.spaces == self.spaces
+        return isinstance(o, ProductSpace) and o.spaces == self.spaces and o._unit == self._unit
 
     def __hash__(self):
         return self._h

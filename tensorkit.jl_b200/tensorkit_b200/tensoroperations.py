@@ -27,6 +27,7 @@ from .spaces import HomSpace, SpaceMismatch
 from .tensor import AdjointTensorMap, TensorMap, new_tensor
 
 __all__ = ["tensoradd_", "tensorcontract_", "tensorcontract", "contract_", "blas_contract_",
+           "tensortrace_", "tensortrace", "tensortrace_structure",
            "tensoradd_structure", "tensorcontract_structure", "tensor", "parse_tensor_expr",
            "adjointtensorindices"]
 
@@ -240,6 +241,30 @@ def parse_tensor_expr(expr):
     return lhs_name, (lcod, ldom), op, factors
 
 
+def tensortrace_structure(A, p, conjA=False) -> HomSpace:
+    """Space of the traced result: select(space(op(A)), p), the structure of tensoradd!
+    (`src/tensors/tensoroperations.jl:72-81`, also used when indices are traced)."""
+    return tensoradd_structure(A, p, conjA)
+
+
+def tensortrace_(C, A, p, q, conjA=False, alpha=1.0, beta=0.0):
+    """TO.tensortrace!(C, A, p, q, conjA, α, β) (`src/tensors/tensoroperations.jl:83-98`):
+    conj(A) through the lazy adjoint with `adjointtensorindices`, then `trace_permute!`."""
+    from .trace import trace_permute_
+    if conjA:
+        Ap = _adjoint(A)
+        p2 = adjointtensorindices(A, _canonicalize(p, C))
+        q2 = adjointtensorindices(A, q)
+        return trace_permute_(C, Ap, p2, q2, alpha, beta)
+    return trace_permute_(C, A, _canonicalize(p, C), q, alpha, beta)
+
+
+def tensortrace(A, p, q, conjA=False, alpha=1.0):
+    """New tensor α·tensortrace(op(A), p, q)."""
+    C = _alloc(tensortrace_structure(A, p, conjA), A)
+    return tensortrace_(C, A, p, q, conjA, alpha, 0.0)
+
+
 def _pairwise_steps(lhs, factors):
     """Plan of pairwise contractions: list of (labelsA, conjA, labelsB, conjB, pA, pB, pAB,
     out_labels, is_final)."""
@@ -270,23 +295,53 @@ def _pairwise_steps(lhs, factors):
     return steps
 
 
+def _trace_labels(labels):
+    """Leg pairs (q₁, q₂) of the labels repeated within one factor (1-based)."""
+    reps = [l for l in dict.fromkeys(labels) if labels.count(l) > 1]
+    for l in reps:
+        if labels.count(l) > 2:
+            raise ValueError(f"label {l!r} appears more than twice in one factor")
+    q1 = tuple(labels.index(l) + 1 for l in reps)
+    q2 = tuple(len(labels) - labels[::-1].index(l) for l in reps)
+    return reps, (q1, q2)
+
+
+def _pretrace(A, labels, conj):
+    """Trace the labels a factor repeats (TensorOperations traces a factor before it enters
+    a contraction); returns the traced tensor and its remaining labels."""
+    reps, q = _trace_labels(labels)
+    if not reps:
+        return A, tuple(labels), conj
+    nout = A.numout()
+    keep = [i for i, l in enumerate(labels) if l not in reps]
+    p = (tuple(i + 1 for i in keep if i < nout), tuple(i + 1 for i in keep if i >= nout))
+    return tensortrace(A, p, q, conj), tuple(labels[i] for i in keep), False
+
+
 def tensor(expr, out=None, alpha=1.0, **tensors):
     """Evaluate an @tensor expression on device TensorMaps.
 
-    `:=` allocates the result; `=` writes into `out` (β = 0); `+=` accumulates (β = 1)."""
+    `:=` allocates the result; `=` writes into `out` (β = 0); `+=` accumulates (β = 1).
+    Labels repeated within one factor are traced (`tensortrace!`)."""
     lhs_name, lhs, op, factors = parse_tensor_expr(expr)
     if len(factors) == 1:
         name, labels, conj = factors[0]
         A = tensors[name]
         lcod, ldom = lhs
         pA = (tuple(labels.index(l) + 1 for l in lcod), tuple(labels.index(l) + 1 for l in ldom))
+        beta = 1.0 if op == "+=" else 0.0
+        reps, q = _trace_labels(labels)
         if out is None:
             out = _alloc(tensoradd_structure(A, pA, conj), A)
-        return tensoradd_(out, A, pA, conj, alpha, 1.0 if op == "+=" else 0.0)
+        if reps:
+            return tensortrace_(out, A, pA, q, conj, alpha, beta)
+        return tensoradd_(out, A, pA, conj, alpha, beta)
+    pre = [_pretrace(tensors[n], lab, cj) for n, lab, cj in factors]
+    factors = [(n, lab, cj) for (n, _, _), (_, lab, cj) in zip(factors, pre)]
     steps = _pairwise_steps(lhs, factors)
-    cur = tensors[factors[0][0]]
+    cur = pre[0][0]
     for i, (la, ca, lb, cb, pA, pB, pAB, outl, final) in enumerate(steps):
-        B = tensors[factors[i + 1][0]]
+        B = pre[i + 1][0]
         if final:
             W = tensorcontract_structure(cur, pA, ca, B, pB, cb, pAB)
             if out is None:

@@ -61,3 +61,28 @@ def test_contraction_via_dense_u1_five_leg():
     C = O.network(fac, (("a", "e"), ("c", "b")), {"A": A, "B": B})
     ref = np.einsum("abcd,de->aecb", D.to_dense(A), D.to_dense(B))
     assert np.abs(D.to_dense(C) - ref).max() < 1e-12 * np.abs(ref).max()
+
+
+@pytest.mark.parametrize("spaces", [VU1, VSU2], ids=["U1", "SU2"])
+def test_trace_via_dense(spaces):
+    """t ∈ V1⊗V2'⊗V3⊗V2⊗V1'⊗V3', t2[a,b] := t[c,d,b,d,c,a] equals the dense partial trace
+    (test/tensors/contractions.jl:60-67)."""
+    V1, V2, V3 = spaces()[:3]
+    W = O.Hom([V1, V2.flipdual(), V3, V2, V1.flipdual(), V3.flipdual()], [])
+    t = O.randn(W, 7, True)
+    t2 = O.trace_permute(t, ((6, 3), ()), ((1, 2), (5, 4)))
+    ref = np.einsum("cdbdca->ab", D.to_dense(t))
+    assert np.abs(D.to_dense(t2) - ref).max() < 1e-12 * np.abs(ref).max()
+
+
+@pytest.mark.parametrize("spaces", [VU1, VSU2, VU1SU2], ids=["U1", "SU2", "U1xSU2"])
+def test_partial_trace_self_consistency(spaces):
+    """t ∈ V1⊗V2⊗V3 ← V1⊗V2⊗V3: t2[a;b] := t[c d b; c d a] equals tracing twice through
+    t4[a b; c d] := t[e d c; e b a], t5[a; b] := t4[a c; b c] (contractions.jl:46-53)."""
+    V1, V2, V3 = spaces()[:3]
+    t = O.randn(O.Hom([V1, V2, V3], [V1, V2, V3]), 8, True)
+    # labels of t: (c, d, b ; c, d, a): legs 1..6
+    t2 = O.trace_permute(t, ((6,), (3,)), ((1, 2), (4, 5)))
+    t4 = O.trace_permute(t, ((6, 5), (3, 2)), ((1,), (4,)))
+    t5 = O.trace_permute(t4, ((1,), (3,)), ((2,), (4,)))
+    assert np.abs(t2.data - t5.data).max() < 1e-12 * np.abs(t2.data).max()
