@@ -49,6 +49,17 @@ struct TGroup {
   int64_t ntile_a, ntile_b;
   int64_t task_begin;
   int64_t src_tree_begin, nsrc, dst_tree_begin, ndst, coeff_begin;
+  // tree 0 only (single-tree groups): strides of the tile dims a and b, coefficient
+  int64_t sa0, sb0, da0, db0;
+  double u0;
+};
+
+// per-task addressing of a single-tree table, resolved on the host
+struct TaskRec {
+  int64_t sbase, dbase;  // element offsets of the tile's first element
+  int32_t na, nb;        // valid extents of the tile
+  int32_t group;
+  int32_t pad;
 };
 
 struct tkb_table {
@@ -58,6 +69,7 @@ struct tkb_table {
   int64_t elems_read = 0, elems_written = 0;
   int max_trees = 1;             // max(nsrc) over groups
   bool single_tree = false;      // every group has one source and one destination tree
+  bool off32 = false;            // every in-tile offset fits 32 bits (both sides)
   size_t smem_f64 = 0;           // dynamic smem bytes needed for f64
   size_t smem_c128 = 0;
   int64_t src_len = 0, dst_len = 0;
@@ -67,6 +79,7 @@ struct tkb_table {
   double *coeffs = nullptr;
   int32_t *task_group = nullptr;  // ntasks: the group of every task
   int32_t *task_idx = nullptr;    // ntasks × (2 + TKB_MAX_IND): tile coordinates, outer index
+  TaskRec *task_rec = nullptr;    // single-tree tables: per-task bases and extents
 };
 
 int tkb_transform_launch(tkb_ctx *ctx, const tkb_table *t, int dtype, void *dst,

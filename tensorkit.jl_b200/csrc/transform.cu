@@ -227,53 +227,6 @@ __global__ void __launch_bounds__(kThreads, sizeof(T) == 8 ? 3 : 2)
 constexpr int kPipeStages = 3;
 constexpr int kStageElems = kTileElemsMax + 256;
 
-struct TaskGeo {
-  int64_t sbase, dbase, sA, sB, dA, dB;
-  int na, nb, ta, lta, ltb, tot, mode, pitch;
-  double u;
-};
-
-__device__ __forceinline__ TaskGeo task_geo(int64_t task, const TGroup *__restrict__ groups,
-                                            const int32_t *__restrict__ task_group,
-                                            const int32_t *__restrict__ task_idx,
-                                            const int64_t *__restrict__ sstr, const int64_t *__restrict__ soff,
-                                            const int64_t *__restrict__ dstr, const int64_t *__restrict__ doff,
-                                            const double *__restrict__ coeffs) {
-  const TGroup &G = groups[task_group[task]];
-  const int32_t *tix = task_idx + task * kTaskWords;
-  const int da = G.da, db = G.db;
-  const int64_t a0 = (int64_t)tix[0] * G.ta, b0 = (int64_t)tix[1] * G.tb;
-  const int64_t *ss = sstr + G.src_tree_begin * TKB_MAX_IND;
-  const int64_t *ds = dstr + G.dst_tree_begin * TKB_MAX_IND;
-  TaskGeo g;
-  g.sA = ss[da];
-  g.dA = ds[da];
-  g.sB = db >= 0 ? ss[db] : 0;
-  g.dB = db >= 0 ? ds[db] : 0;
-  int64_t so = soff[G.src_tree_begin] + a0 * g.sA + b0 * g.sB;
-  int64_t dof = doff[G.dst_tree_begin] + a0 * g.dA + b0 * g.dB;
-#pragma unroll
-  for (int q = 0; q < TKB_MAX_IND; ++q)
-    if (q < G.nouter) {
-      const int64_t o = tix[2 + q];
-      so += o * ss[G.outer[q]];
-      dof += o * ds[G.outer[q]];
-    }
-  g.sbase = so;
-  g.dbase = dof;
-  const int64_t sa = G.size[da], sb = db >= 0 ? G.size[db] : 1;
-  g.na = (int)(sa - a0 < G.ta ? sa - a0 : G.ta);
-  g.nb = (int)(sb - b0 < G.tb ? sb - b0 : G.tb);
-  g.ta = G.ta;
-  g.lta = __ffs(G.ta) - 1;
-  g.ltb = __ffs(G.tb) - 1;
-  g.tot = G.ta * G.tb;
-  g.mode = G.mode;
-  g.pitch = G.tb + 1;
-  g.u = coeffs[G.coeff_begin];
-  return g;
-}
-
 __device__ __forceinline__ void cp_async_el(double *sm, const double *g) {
   asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"((unsigned)__cvta_generic_to_shared(sm)),
                "l"(g)
@@ -295,14 +248,13 @@ __device__ __forceinline__ double2 conj_v(double2 v, bool c) {
   return v;
 }
 
-template <typename T, bool CONJ>
+// OFF: the integer type of in-tile offsets (32-bit when every tile's span fits, which keeps
+// the per-element address arithmetic to single-word multiply-adds)
+template <typename T, bool CONJ, typename OFF>
 __global__ void __launch_bounds__(kThreads)
-    treetransform_pipe_kernel(const TGroup *__restrict__ groups, const int32_t *__restrict__ task_group,
-                              const int32_t *__restrict__ task_idx, int64_t ntasks,
-                              const int64_t *__restrict__ sstr, const int64_t *__restrict__ soff,
-                              const int64_t *__restrict__ dstr, const int64_t *__restrict__ doff,
-                              const double *__restrict__ coeffs, T *__restrict__ dst,
-                              const T *__restrict__ src, CDbl alpha_, CDbl beta_, int beta_zero) {
+    treetransform_pipe_kernel(const TGroup *__restrict__ groups, const TaskRec *__restrict__ recs,
+                              int64_t ntasks, T *__restrict__ dst, const T *__restrict__ src, CDbl alpha_,
+                              CDbl beta_, int beta_zero) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   T *sm = reinterpret_cast<T *>(smem_raw);
   const T alpha = scalar_from<T>(alpha_);
@@ -313,32 +265,40 @@ __global__ void __launch_bounds__(kThreads)
   const int64_t t_end = min(ntasks, t_begin + per);
 
   auto issue = [&](int64_t task, T *stage) {
-    const TaskGeo g = task_geo(task, groups, task_group, task_idx, sstr, soff, dstr, doff, coeffs);
-    for (int e = threadIdx.x; e < g.tot; e += kThreads) {
-      int ia, ib, si;
-      if (g.mode == 1) {  // source-fast b: coalesced reads, tile stored row-pitched
-        ia = e >> g.ltb;
-        ib = e & ((1 << g.ltb) - 1);
-        si = ia * g.pitch + ib;
-      } else {
-        ia = e & (g.ta - 1);
-        ib = e >> g.lta;
-        si = ib * g.ta + ia;
+    const TaskRec R = recs[task];
+    const TGroup &G = groups[R.group];
+    const int ta = G.ta, tot = G.ta * G.tb, lta = __ffs(G.ta) - 1, ltb = __ffs(G.tb) - 1;
+    const OFF sA = (OFF)G.sa0, sB = (OFF)G.sb0;
+    const T *sb = src + R.sbase;
+    if (G.mode == 1) {  // source-fast b: coalesced reads, tile stored row-pitched (tb + 1)
+      for (int e = threadIdx.x; e < tot; e += kThreads) {
+        const int ia = e >> ltb, ib = e & ((1 << ltb) - 1);
+        if (ia < R.na && ib < R.nb) cp_async_el(stage + ia * (G.tb + 1) + ib, sb + (OFF)ia * sA + (OFF)ib * sB);
       }
-      if (ia < g.na && ib < g.nb) cp_async_el(stage + si, src + g.sbase + ia * g.sA + ib * g.sB);
+    } else {
+      for (int e = threadIdx.x; e < tot; e += kThreads) {
+        const int ia = e & (ta - 1), ib = e >> lta;
+        if (ia < R.na && ib < R.nb) cp_async_el(stage + e, sb + (OFF)ia * sA + (OFF)ib * sB);
+      }
     }
   };
   auto write = [&](int64_t task, const T *stage) {
-    const TaskGeo g = task_geo(task, groups, task_group, task_idx, sstr, soff, dstr, doff, coeffs);
-    for (int e0 = 0; e0 < g.tot; e0 += kThreads * kBatch) {
+    const TaskRec R = recs[task];
+    const TGroup &G = groups[R.group];
+    const int ta = G.ta, tot = G.ta * G.tb, lta = __ffs(G.ta) - 1;
+    const int pitch = G.mode == 1 ? G.tb + 1 : 0;
+    const OFF dA = (OFF)G.da0, dB = (OFF)G.db0;
+    const double u = G.u0;
+    T *db = dst + R.dbase;
+    for (int e0 = 0; e0 < tot; e0 += kThreads * kBatch) {
 #pragma unroll
       for (int q = 0; q < kBatch; ++q) {
         const int e = e0 + q * kThreads + threadIdx.x;
-        const int ia = e & (g.ta - 1), ib = e >> g.lta;  // a fastest: coalesced writes
-        if (e < g.tot && ia < g.na && ib < g.nb) {
-          const T v = conj_v(stage[g.mode == 1 ? ia * g.pitch + ib : ib * g.ta + ia], CONJ);
-          T *dp = dst + g.dbase + ia * g.dA + ib * g.dB;
-          *dp = finish(axpy_r(g.u, v, zero_val(T{})), alpha, beta, dp, bz);
+        const int ia = e & (ta - 1), ib = e >> lta;  // a fastest: coalesced writes
+        if (e < tot && ia < R.na && ib < R.nb) {
+          const T v = conj_v(stage[pitch ? ia * pitch + ib : e], CONJ);
+          T *dp = db + (OFF)ia * dA + (OFF)ib * dB;
+          *dp = finish(axpy_r(u, v, zero_val(T{})), alpha, beta, dp, bz);
         }
       }
     }
@@ -399,6 +359,8 @@ extern "C" int tkb_table_create(tkb_ctx *ctx, const tkb_table_desc *d, tkb_table
   std::vector<int64_t> hsstr, hsoff, hdstr, hdoff;
   std::vector<int32_t> htask;  // task → group
   std::vector<int32_t> hidx;   // task → (tile a, tile b, outer multi-index)
+  std::vector<TaskRec> hrec;   // task → tree-0 bases and extents (single-tree tables)
+  bool all_off32 = true;
   std::vector<double> hcoef;
   int64_t ntasks = 0, er = 0, ew = 0;
   size_t smem_max_f64 = 0, smem_max_c128 = 0;
@@ -575,6 +537,16 @@ extern "C" int tkb_table_create(tkb_ctx *ctx, const tkb_table_desc *d, tkb_table
     }
     max_trees = std::max<int>(max_trees, (int)nsrc);
     max_dst = std::max<int>(max_dst, (int)ndst);
+    tg.sa0 = dims[fa].ss[0];
+    tg.da0 = dims[fa].ds[0];
+    tg.sb0 = db >= 0 ? dims[db].ss[0] : 0;
+    tg.db0 = db >= 0 ? dims[db].ds[0] : 0;
+    tg.u0 = d->coeffs[c0];
+    {
+      const int64_t lim = (int64_t)INT32_MAX;
+      const int64_t so = (ta - 1) * tg.sa0 + (tb - 1) * tg.sb0, dso = (ta - 1) * tg.da0 + (tb - 1) * tg.db0;
+      if (tg.sa0 > lim || tg.sb0 > lim || tg.da0 > lim || tg.db0 > lim || so > lim || dso > lim) all_off32 = false;
+    }
     htask.insert(htask.end(), (size_t)(ntasks - tg.task_begin), (int32_t)g);
     for (int64_t t = 0; t < ntasks - tg.task_begin; ++t) {
       int64_t r = t;
@@ -589,6 +561,22 @@ extern "C" int tkb_table_create(tkb_ctx *ctx, const tkb_table_desc *d, tkb_table
         r /= sq;
       }
       hidx.insert(hidx.end(), w, w + kTaskWords);
+      if (nsrc == 1 && ndst == 1) {
+        const int64_t a0 = (int64_t)w[0] * ta, b0 = (int64_t)w[1] * tb;
+        TaskRec rec;
+        rec.sbase = d->src_offsets[s0] + a0 * tg.sa0 + b0 * tg.sb0;
+        rec.dbase = d->dst_offsets[t0] + a0 * tg.da0 + b0 * tg.db0;
+        for (int q = 0; q < tg.nouter; ++q) {
+          rec.sbase += (int64_t)w[2 + q] * dims[tg.outer[q]].ss[0];
+          rec.dbase += (int64_t)w[2 + q] * dims[tg.outer[q]].ds[0];
+        }
+        const int64_t sa = dims[fa].size, sb = db >= 0 ? dims[db].size : 1;
+        rec.na = (int32_t)std::min<int64_t>(ta, sa - a0);
+        rec.nb = (int32_t)std::min<int64_t>(tb, sb - b0);
+        rec.group = (int32_t)g;
+        rec.pad = 0;
+        hrec.push_back(rec);
+      }
     }
     hg.push_back(tg);
   }
@@ -603,6 +591,7 @@ extern "C" int tkb_table_create(tkb_ctx *ctx, const tkb_table_desc *d, tkb_table
   t->elems_written = ew;
   t->max_trees = max_trees;
   t->single_tree = max_trees == 1 && max_dst == 1;
+  t->off32 = all_off32;
   t->smem_f64 = smem_max_f64;
   t->smem_c128 = smem_max_c128;
   t->src_len = d->src_len;
@@ -617,6 +606,7 @@ extern "C" int tkb_table_create(tkb_ctx *ctx, const tkb_table_desc *d, tkb_table
   if (e == cudaSuccess) e = up((void **)&t->groups, hg.data(), hg.size() * sizeof(TGroup));
   if (e == cudaSuccess) e = up((void **)&t->task_group, htask.data(), htask.size() * 4);
   if (e == cudaSuccess) e = up((void **)&t->task_idx, hidx.data(), hidx.size() * 4);
+  if (e == cudaSuccess && t->single_tree) e = up((void **)&t->task_rec, hrec.data(), hrec.size() * sizeof(TaskRec));
   if (e == cudaSuccess) e = up((void **)&t->sstr, hsstr.data(), hsstr.size() * 8);
   if (e == cudaSuccess) e = up((void **)&t->soff, hsoff.data(), hsoff.size() * 8);
   if (e == cudaSuccess) e = up((void **)&t->dstr, hdstr.data(), hdstr.size() * 8);
@@ -636,6 +626,7 @@ extern "C" int tkb_table_destroy(tkb_table *t) {
   cudaFree(t->groups);
   cudaFree(t->task_group);
   cudaFree(t->task_idx);
+  cudaFree(t->task_rec);
   cudaFree(t->sstr);
   cudaFree(t->soff);
   cudaFree(t->dstr);
@@ -667,16 +658,18 @@ int tkb_transform_launch(tkb_ctx *ctx, const tkb_table *t, int dtype, void *dst,
     const size_t smem = (size_t)kPipeStages * kStageElems * el;
     const int pgrid = (int)std::min<int64_t>(t->ntasks, (int64_t)ctx->num_sms * (dtype == TKB_F64 ? 4 : 2));
     if (dtype == TKB_F64) {
-      auto k = treetransform_pipe_kernel<double, false>;
+      auto k = t->off32 ? treetransform_pipe_kernel<double, false, int32_t>
+                        : treetransform_pipe_kernel<double, false, int64_t>;
       TKB_CUDA_TRY(ctx, cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-      k<<<pgrid, kThreads, smem, ctx->stream>>>(t->groups, t->task_group, t->task_idx, t->ntasks, t->sstr,
-                                               t->soff, t->dstr, t->doff, t->coeffs, (double *)dst,
+      k<<<pgrid, kThreads, smem, ctx->stream>>>(t->groups, t->task_rec, t->ntasks, (double *)dst,
                                                (const double *)src, a, b, bz);
     } else {
-      auto k = conj ? treetransform_pipe_kernel<double2, true> : treetransform_pipe_kernel<double2, false>;
+      auto k = conj ? (t->off32 ? treetransform_pipe_kernel<double2, true, int32_t>
+                                : treetransform_pipe_kernel<double2, true, int64_t>)
+                    : (t->off32 ? treetransform_pipe_kernel<double2, false, int32_t>
+                                : treetransform_pipe_kernel<double2, false, int64_t>);
       TKB_CUDA_TRY(ctx, cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-      k<<<pgrid, kThreads, smem, ctx->stream>>>(t->groups, t->task_group, t->task_idx, t->ntasks, t->sstr,
-                                               t->soff, t->dstr, t->doff, t->coeffs, (double2 *)dst,
+      k<<<pgrid, kThreads, smem, ctx->stream>>>(t->groups, t->task_rec, t->ntasks, (double2 *)dst,
                                                (const double2 *)src, a, b, bz);
     }
     ctx->launches++;
