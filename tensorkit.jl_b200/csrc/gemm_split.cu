@@ -67,6 +67,13 @@ __device__ __noinline__ double ldexp_slow(double v, int e) { return ldexp(v, e);
 __device__ __forceinline__ double scale2(double v, int e) {
   return (e >= -1022 && e <= 1023) ? v * pow2i(e) : ldexp_slow(v, e);
 }
+// v·2^e without a call: e split into two normal exponents (exact for every e reachable from
+// two row/column exponents; only a result in the subnormal range can round twice)
+__device__ __forceinline__ double scale2_inline(double v, int e) {
+  const int e1 = min(max(e, -1022), 1023);
+  const int e2 = min(max(e - e1, -1022), 1023);
+  return v * pow2i(e1) * pow2i(e2);
+}
 // exact int64 → double for |x| < 2^51: x is added to the mantissa of 1.5·2^52 (whose unit in
 // the last place is 1), and 1.5·2^52 is subtracted again
 __device__ __forceinline__ double i2d_small(int64_t x) {
@@ -709,7 +716,7 @@ __global__ void __launch_bounds__(128, 1)
   auto final_store = [&](int c, const double (&v)[16]) {
     double r[16];
 #pragma unroll
-    for (int q = 0; q < 16; ++q) r[q] = has_k ? scale2(v[q], ei + ebs[c * 16 + q]) : v[q];
+    for (int q = 0; q < 16; ++q) r[q] = has_k ? scale2_inline(v[q], ei + ebs[c * 16 + q]) : v[q];
     if (!cplx) {
       const int64_t j0 = tile.n0 + c * 16;
       const int nj = (int)min((int64_t)16, b.n - j0);

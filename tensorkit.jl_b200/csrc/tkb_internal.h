@@ -54,12 +54,14 @@ struct TGroup {
   double u0;
 };
 
-// per-task addressing of a single-tree table, resolved on the host
+// complete addressing of one task of a single-tree table, resolved on the host (80 bytes)
 struct TaskRec {
-  int64_t sbase, dbase;  // element offsets of the tile's first element
-  int32_t na, nb;        // valid extents of the tile
-  int32_t group;
-  int32_t pad;
+  int64_t sbase, dbase;      // element offsets of the tile's first element
+  int64_t sA, sB, dA, dB;    // strides of the tile dims on both sides
+  double u;                  // recoupling coefficient
+  int32_t na, nb;            // valid extents of the tile
+  int32_t ta, tb;            // tile extents (powers of two)
+  int32_t mode, pad;
 };
 
 struct tkb_table {

@@ -249,53 +249,65 @@ __device__ __forceinline__ double2 conj_v(double2 v, bool c) {
 }
 
 // OFF: the integer type of in-tile offsets (32-bit when every tile's span fits, which keeps
-// the per-element address arithmetic to single-word multiply-adds)
+// the per-element address arithmetic to single-word multiply-adds). The records of the CTA's
+// tasks (at most kRecCache) are copied to shared memory first, so no task waits on a
+// dependent metadata load.
+constexpr int kRecCache = 64;
+
 template <typename T, bool CONJ, typename OFF>
 __global__ void __launch_bounds__(kThreads)
-    treetransform_pipe_kernel(const TGroup *__restrict__ groups, const TaskRec *__restrict__ recs,
-                              int64_t ntasks, T *__restrict__ dst, const T *__restrict__ src, CDbl alpha_,
-                              CDbl beta_, int beta_zero) {
+    treetransform_pipe_kernel(const TaskRec *__restrict__ recs, int64_t ntasks, T *__restrict__ dst,
+                              const T *__restrict__ src, CDbl alpha_, CDbl beta_, int beta_zero) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
+  __shared__ TaskRec rs[kRecCache];
   T *sm = reinterpret_cast<T *>(smem_raw);
   const T alpha = scalar_from<T>(alpha_);
   const T beta = scalar_from<T>(beta_);
   const bool bz = beta_zero != 0;
-  const int64_t per = (ntasks + gridDim.x - 1) / gridDim.x;
+  const int64_t per = (ntasks + gridDim.x - 1) / gridDim.x;  // ≤ kRecCache (host)
   const int64_t t_begin = (int64_t)blockIdx.x * per;
   const int64_t t_end = min(ntasks, t_begin + per);
+  {
+    const int nw = (int)(t_end > t_begin ? t_end - t_begin : 0) * (int)(sizeof(TaskRec) / 8);
+    const int64_t *srcw = reinterpret_cast<const int64_t *>(recs + t_begin);
+    int64_t *dstw = reinterpret_cast<int64_t *>(rs);
+    for (int i = threadIdx.x; i < nw; i += kThreads) dstw[i] = __ldg(srcw + i);
+  }
+  __syncthreads();
 
   auto issue = [&](int64_t task, T *stage) {
-    const TaskRec R = recs[task];
-    const TGroup &G = groups[R.group];
-    const int ta = G.ta, tot = G.ta * G.tb, lta = __ffs(G.ta) - 1, ltb = __ffs(G.tb) - 1;
-    const OFF sA = (OFF)G.sa0, sB = (OFF)G.sb0;
+    const TaskRec &R = rs[task - t_begin];
+    const int ta = R.ta, tot = R.ta * R.tb, lta = __ffs(R.ta) - 1, ltb = __ffs(R.tb) - 1;
+    const OFF sA = (OFF)R.sA, sB = (OFF)R.sB;
+    const int na = R.na, nb = R.nb;
     const T *sb = src + R.sbase;
-    if (G.mode == 1) {  // source-fast b: coalesced reads, tile stored row-pitched (tb + 1)
+    if (R.mode == 1) {  // source-fast b: coalesced reads, tile stored row-pitched (tb + 1)
+      const int pitch = R.tb + 1;
       for (int e = threadIdx.x; e < tot; e += kThreads) {
         const int ia = e >> ltb, ib = e & ((1 << ltb) - 1);
-        if (ia < R.na && ib < R.nb) cp_async_el(stage + ia * (G.tb + 1) + ib, sb + (OFF)ia * sA + (OFF)ib * sB);
+        if (ia < na && ib < nb) cp_async_el(stage + ia * pitch + ib, sb + (OFF)ia * sA + (OFF)ib * sB);
       }
     } else {
       for (int e = threadIdx.x; e < tot; e += kThreads) {
         const int ia = e & (ta - 1), ib = e >> lta;
-        if (ia < R.na && ib < R.nb) cp_async_el(stage + e, sb + (OFF)ia * sA + (OFF)ib * sB);
+        if (ia < na && ib < nb) cp_async_el(stage + e, sb + (OFF)ia * sA + (OFF)ib * sB);
       }
     }
   };
   auto write = [&](int64_t task, const T *stage) {
-    const TaskRec R = recs[task];
-    const TGroup &G = groups[R.group];
-    const int ta = G.ta, tot = G.ta * G.tb, lta = __ffs(G.ta) - 1;
-    const int pitch = G.mode == 1 ? G.tb + 1 : 0;
-    const OFF dA = (OFF)G.da0, dB = (OFF)G.db0;
-    const double u = G.u0;
+    const TaskRec &R = rs[task - t_begin];
+    const int ta = R.ta, tot = R.ta * R.tb, lta = __ffs(R.ta) - 1;
+    const int pitch = R.mode == 1 ? R.tb + 1 : 0;
+    const OFF dA = (OFF)R.dA, dB = (OFF)R.dB;
+    const int na = R.na, nb = R.nb;
+    const double u = R.u;
     T *db = dst + R.dbase;
     for (int e0 = 0; e0 < tot; e0 += kThreads * kBatch) {
 #pragma unroll
       for (int q = 0; q < kBatch; ++q) {
         const int e = e0 + q * kThreads + threadIdx.x;
         const int ia = e & (ta - 1), ib = e >> lta;  // a fastest: coalesced writes
-        if (e < tot && ia < R.na && ib < R.nb) {
+        if (e < tot && ia < na && ib < nb) {
           const T v = conj_v(stage[pitch ? ia * pitch + ib : e], CONJ);
           T *dp = db + (OFF)ia * dA + (OFF)ib * dB;
           *dp = finish(axpy_r(u, v, zero_val(T{})), alpha, beta, dp, bz);
@@ -573,7 +585,14 @@ extern "C" int tkb_table_create(tkb_ctx *ctx, const tkb_table_desc *d, tkb_table
         const int64_t sa = dims[fa].size, sb = db >= 0 ? dims[db].size : 1;
         rec.na = (int32_t)std::min<int64_t>(ta, sa - a0);
         rec.nb = (int32_t)std::min<int64_t>(tb, sb - b0);
-        rec.group = (int32_t)g;
+        rec.sA = tg.sa0;
+        rec.sB = tg.sb0;
+        rec.dA = tg.da0;
+        rec.dB = tg.db0;
+        rec.u = tg.u0;
+        rec.ta = (int32_t)ta;
+        rec.tb = (int32_t)tb;
+        rec.mode = tg.mode;
         rec.pad = 0;
         hrec.push_back(rec);
       }
@@ -653,25 +672,36 @@ int tkb_transform_launch(tkb_ctx *ctx, const tkb_table *t, int dtype, void *dst,
   if (t->single_tree && (dtype == TKB_F64 || dtype == TKB_C128) && !use_plain_transform()) {
     if (dtype == TKB_F64 && (alpha.im != 0.0 || beta.im != 0.0))
       return tkb_set_error(ctx, TKB_ERR_ARG, "complex scalar with real data");
-    // persistent CTAs, as many as the stage ring lets reside (4 real / 2 complex per SM)
+    // persistent CTAs: as many as reside at once (occupancy of the stage ring), with at most
+    // kRecCache tasks each
     const size_t el = dtype == TKB_F64 ? 8 : 16;
     const size_t smem = (size_t)kPipeStages * kStageElems * el;
-    const int pgrid = (int)std::min<int64_t>(t->ntasks, (int64_t)ctx->num_sms * (dtype == TKB_F64 ? 4 : 2));
+    using KD = void (*)(const TaskRec *, int64_t, double *, const double *, CDbl, CDbl, int);
+    using KC = void (*)(const TaskRec *, int64_t, double2 *, const double2 *, CDbl, CDbl, int);
+    KD kd = nullptr;
+    KC kc = nullptr;
+    const void *kfn;
     if (dtype == TKB_F64) {
-      auto k = t->off32 ? treetransform_pipe_kernel<double, false, int32_t>
-                        : treetransform_pipe_kernel<double, false, int64_t>;
-      TKB_CUDA_TRY(ctx, cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-      k<<<pgrid, kThreads, smem, ctx->stream>>>(t->groups, t->task_rec, t->ntasks, (double *)dst,
-                                               (const double *)src, a, b, bz);
+      kd = t->off32 ? treetransform_pipe_kernel<double, false, int32_t> : treetransform_pipe_kernel<double, false, int64_t>;
+      kfn = (const void *)kd;
     } else {
-      auto k = conj ? (t->off32 ? treetransform_pipe_kernel<double2, true, int32_t>
-                                : treetransform_pipe_kernel<double2, true, int64_t>)
-                    : (t->off32 ? treetransform_pipe_kernel<double2, false, int32_t>
-                                : treetransform_pipe_kernel<double2, false, int64_t>);
-      TKB_CUDA_TRY(ctx, cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-      k<<<pgrid, kThreads, smem, ctx->stream>>>(t->groups, t->task_rec, t->ntasks, (double2 *)dst,
-                                               (const double2 *)src, a, b, bz);
+      kc = conj ? (t->off32 ? treetransform_pipe_kernel<double2, true, int32_t>
+                            : treetransform_pipe_kernel<double2, true, int64_t>)
+                : (t->off32 ? treetransform_pipe_kernel<double2, false, int32_t>
+                            : treetransform_pipe_kernel<double2, false, int64_t>);
+      kfn = (const void *)kc;
     }
+    TKB_CUDA_TRY(ctx, cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    int per_sm = 1;
+    TKB_CUDA_TRY(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kfn, kThreads, smem));
+    int64_t pg = std::min<int64_t>(t->ntasks, (int64_t)ctx->num_sms * std::max(1, per_sm));
+    pg = std::max<int64_t>(pg, (t->ntasks + kRecCache - 1) / kRecCache);
+    const int pgrid = (int)pg;
+    if (kd)
+      kd<<<pgrid, kThreads, smem, ctx->stream>>>(t->task_rec, t->ntasks, (double *)dst, (const double *)src, a, b, bz);
+    else
+      kc<<<pgrid, kThreads, smem, ctx->stream>>>(t->task_rec, t->ntasks, (double2 *)dst, (const double2 *)src, a, b,
+                                                 bz);
     ctx->launches++;
     TKB_CUDA_TRY(ctx, cudaGetLastError());
     return TKB_OK;
