@@ -417,6 +417,8 @@ __global__ void __launch_bounds__(kSliceThreads, CPLX ? 1 : 2)
   extern __shared__ __align__(16) unsigned char slice_smem[];
   __shared__ unsigned long long rmax[32];
   __shared__ int rexp[32];
+  pdl_wait();     // the operands come from the previous kernel of the stream
+  pdl_trigger();  // the product kernel may be scheduled (it waits for this grid to finish)
   const SliceTask task = tasks[blockIdx.x / cluster_size()];
   const GBlock &b = blocks[task.block];
   const int op = task.operand;
@@ -596,6 +598,7 @@ __global__ void __launch_bounds__(128, 1)
   __syncthreads();
   tc_fence_after();
   const uint32_t tmem = has_k ? *tmem_slot : 0u;
+  pdl_wait();  // slices and exponents come from the slicing kernel (set-up above overlapped it)
   if (tid >= 64) {  // column exponents into shared memory while warp 0 starts the products
     const int col = tid - 64;
     const int64_t j = tile.n0 + col;
@@ -954,13 +957,15 @@ int launch_split(tkb_ctx *ctx, const tkb_plan *p, void *C, const void *A, const 
     cfg.blockDim = dim3(kSliceThreads);
     cfg.dynamicSmemBytes = smem;
     cfg.stream = ctx->stream;
-    cudaLaunchAttribute attr[1];
+    cudaLaunchAttribute attr[2];
     attr[0].id = cudaLaunchAttributeClusterDimension;
     attr[0].val.clusterDim.x = cs;
     attr[0].val.clusterDim.y = 1;
     attr[0].val.clusterDim.z = 1;
+    attr[1].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[1].val.programmaticStreamSerializationAllowed = 1;
     cfg.attrs = attr;
-    cfg.numAttrs = 1;
+    cfg.numAttrs = 2;
     TKB_CUDA_TRY(ctx, cudaLaunchKernelEx(&cfg, k, (const GBlock *)p->blocks, (const SliceTask *)p->sjobs,
                                          (const double *)A, (const double *)B, (int8_t *)ctx->ws));
     ctx->launches++;
@@ -980,9 +985,20 @@ int launch_split(tkb_ctx *ctx, const tkb_plan *p, void *C, const void *A, const 
     const size_t smem = ring_stages(S) * (size_t)S * (PANEL_A + PANEL_B) * KSTAGE + 512;
     auto k = gemm_split_tc_kernel<S>;
     TKB_CUDA_TRY(ctx, cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    k<<<(int)p->nkstiles, 128, smem, ctx->stream>>>(p->blocks, (const SplitTile *)p->kstiles,
-                                                    (const int8_t *)ctx->ws, cplx, (double *)C, a, b,
-                                                    ctx->counters + 8, p->part, p->pcnt);
+    // programmatic dependent launch: barrier set-up and TMEM allocation overlap the slicing
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)p->nkstiles);
+    cfg.blockDim = dim3(128);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = ctx->stream;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = p->nsrows > 0 ? 1 : 0;
+    TKB_CUDA_TRY(ctx, cudaLaunchKernelEx(&cfg, k, (const GBlock *)p->blocks, (const SplitTile *)p->kstiles,
+                                         (const int8_t *)ctx->ws, cplx, (double *)C, a, b, ctx->counters + 8,
+                                         p->part, p->pcnt));
   }
   ctx->launches++;
   TKB_CUDA_TRY(ctx, cudaGetLastError());

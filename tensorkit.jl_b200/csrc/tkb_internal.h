@@ -25,6 +25,15 @@ struct tkb_ctx {
   bool in_capture = false;
 };
 
+// programmatic dependent launch: a kernel launched with the programmatic-serialization
+// attribute may start while the previous kernel of the stream still runs; it must call
+// pdl_wait() before touching anything that kernel writes (a no-op without the attribute).
+// pdl_trigger() lets the next kernel be scheduled once every CTA of this one has called it.
+#ifdef __CUDACC__
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;\n" ::: "memory"); }
+__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;\n" ::: "memory"); }
+#endif
+
 // status helpers ------------------------------------------------------------------------
 int tkb_set_error(tkb_ctx *ctx, int code, const std::string &msg);
 #define TKB_CUDA_TRY(ctx, call)                                                            \

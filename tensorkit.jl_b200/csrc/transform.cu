@@ -86,6 +86,7 @@ __global__ void __launch_bounds__(kThreads, sizeof(T) == 8 ? 3 : 2)
   const T alpha = scalar_from<T>(alpha_);
   const T beta = scalar_from<T>(beta_);
   const bool bz = beta_zero != 0;
+  pdl_trigger();  // the next kernel may be scheduled; it waits for this grid before reading
 
   // Each CTA walks a contiguous range of tasks (tasks of one group are contiguous, so the
   // group metadata stays in L1); the task → group map was built on the host.
@@ -264,6 +265,7 @@ __global__ void __launch_bounds__(kThreads)
   const T alpha = scalar_from<T>(alpha_);
   const T beta = scalar_from<T>(beta_);
   const bool bz = beta_zero != 0;
+  pdl_trigger();  // the next kernel may be scheduled; it waits for this grid before reading
   const int64_t per = (ntasks + gridDim.x - 1) / gridDim.x;  // ≤ kRecCache (host)
   const int64_t t_begin = (int64_t)blockIdx.x * per;
   const int64_t t_end = min(ntasks, t_begin + per);
