@@ -48,8 +48,8 @@ constexpr int KSTAGE = 32;                   // bytes of K per stage (one tensor
 constexpr int kSmemMax = 232448;             // dynamic shared memory per CTA (227 KiB)
 // depth of the shared-memory ring: as many stages of S slices of A and B as fit, at most 8
 __host__ __device__ constexpr int ring_stages(int S) {
-  return (kSmemMax - 512) / (S * (PANEL_A + PANEL_B) * KSTAGE) < 8
-             ? (kSmemMax - 512) / (S * (PANEL_A + PANEL_B) * KSTAGE)
+  return (kSmemMax - 1024) / (S * (PANEL_A + PANEL_B) * KSTAGE) < 8
+             ? (kSmemMax - 1024) / (S * (PANEL_A + PANEL_B) * KSTAGE)
              : 8;
 }
 constexpr int SMAX = 7;
@@ -66,13 +66,6 @@ __device__ __noinline__ double ldexp_slow(double v, int e) { return ldexp(v, e);
 // v·2^e: one exact multiplication when 2^e is a normal number, else ldexp
 __device__ __forceinline__ double scale2(double v, int e) {
   return (e >= -1022 && e <= 1023) ? v * pow2i(e) : ldexp_slow(v, e);
-}
-// v·2^e without a call: e split into two normal exponents (exact for every e reachable from
-// two row/column exponents; only a result in the subnormal range can round twice)
-__device__ __forceinline__ double scale2_inline(double v, int e) {
-  const int e1 = min(max(e, -1022), 1023);
-  const int e2 = min(max(e - e1, -1022), 1023);
-  return v * pow2i(e1) * pow2i(e2);
 }
 // exact int64 → double for |x| < 2^51: x is added to the mantissa of 1.5·2^52 (whose unit in
 // the last place is 1), and 1.5·2^52 is subtracted again
@@ -572,6 +565,7 @@ __global__ void __launch_bounds__(128, 1)
   uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(full + 2 * NSTAGE + 1);
   int *ticket = reinterpret_cast<int *>(full + 2 * NSTAGE + 2);
   int *ebs = reinterpret_cast<int *>(full + 2 * NSTAGE + 4);  // column exponents of the tile
+  double *cscale = reinterpret_cast<double *>(full + 2 * NSTAGE + 36);  // 2^(column exponent)
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const SplitTile tile = tiles[blockIdx.x];
   const GBlock b = blocks[tile.block];
@@ -602,7 +596,9 @@ __global__ void __launch_bounds__(128, 1)
   if (tid >= 64) {  // column exponents into shared memory while warp 0 starts the products
     const int col = tid - 64;
     const int64_t j = tile.n0 + col;
-    ebs[col] = (has_k && j < b.n) ? max(reinterpret_cast<const int32_t *>(ws + b.wsEB)[j], -1100) : 0;
+    const int ej = (has_k && j < b.n) ? max(reinterpret_cast<const int32_t *>(ws + b.wsEB)[j], -1100) : 0;
+    ebs[col] = ej;
+    cscale[col] = (ej >= -1022 && ej <= 1023) ? pow2i(ej) : 0.0;  // 0: scale through ldexp
   }
 
   // producer: lane 0 of warp 0; the other lanes of warp 0 wait at the __syncwarp below (no
@@ -683,6 +679,7 @@ __global__ void __launch_bounds__(128, 1)
   const int row = 32 * warp + lane;
   const int64_t i = tile.m0 + row;
   const int ei = (has_k && i < Mreal) ? max(eA[i], -1100) : 0;
+  const double rscale = (ei >= -1022 && ei <= 1023) ? pow2i(ei) : 0.0;
   // this CTA's FP64 recombination of its diagonals: chunk c of 16 columns
   auto recombine = [&](int c, double (&v)[16]) {
 #pragma unroll
@@ -714,55 +711,63 @@ __global__ void __launch_bounds__(128, 1)
       v[q] = acc;
     }
   };
+  // Every row exponent and column exponent of the tile in the normal range (the common case):
+  // the final scaling is two exact multiplications by powers of two; otherwise ldexp.
+  int any_slow = (has_k && rscale == 0.0) ? 1 : 0;
+  if (has_k && lane < 16 && warp == 0)
+    any_slow |= (cscale[4 * lane] == 0.0 || cscale[4 * lane + 1] == 0.0 || cscale[4 * lane + 2] == 0.0 ||
+                 cscale[4 * lane + 3] == 0.0) ? 1 : 0;
+  const bool slow = __syncthreads_or(any_slow) != 0;
   // final values of chunk c: exponent scaling, α/β update, store to C (real: every old
   // value of C is loaded before the first store, so no load waits behind a store)
-  auto final_store = [&](int c, const double (&v)[16]) {
-    double r[16];
+  auto final_store = [&](int c, double (&v)[16]) {
+    if (has_k) {
+      if (!slow) {
 #pragma unroll
-    for (int q = 0; q < 16; ++q) r[q] = has_k ? scale2_inline(v[q], ei + ebs[c * 16 + q]) : v[q];
+        for (int q = 0; q < 16; ++q) v[q] = v[q] * rscale * cscale[c * 16 + q];
+      } else {
+#pragma unroll
+        for (int q = 0; q < 16; ++q) v[q] = scale2(v[q], ei + ebs[c * 16 + q]);
+      }
+    }
     if (!cplx) {
       const int64_t j0 = tile.n0 + c * 16;
       const int nj = (int)min((int64_t)16, b.n - j0);
       if (i >= b.m || nj <= 0) return;
       double *pc = C + b.offC + i + j0 * b.ldc;
-      double old[16];
+      if (bz) {
 #pragma unroll
-      for (int q = 0; q < 16; ++q) old[q] = (!bz && q < nj) ? pc[q * b.ldc] : 0.0;
+        for (int q = 0; q < 16; ++q)
+          if (q < nj) pc[q * b.ldc] = alpha.x * v[q];
+      } else {
+        double old[16];
 #pragma unroll
-      for (int q = 0; q < 16; ++q)
-        if (q < nj) pc[q * b.ldc] = bz ? alpha.x * r[q] : fma(beta.x, old[q], alpha.x * r[q]);
+        for (int q = 0; q < 16; ++q) old[q] = q < nj ? pc[q * b.ldc] : 0.0;
+#pragma unroll
+        for (int q = 0; q < 16; ++q)
+          if (q < nj) pc[q * b.ldc] = fma(beta.x, old[q], alpha.x * v[q]);
+      }
       return;
     }
 #pragma unroll
-    for (int q = 0; q < 16; ++q) store_out(r[q], i, tile.n0 + c * 16 + q, b, cplx, C, alpha, beta, bz, 1);
+    for (int q = 0; q < 16; ++q) store_out(v[q], i, tile.n0 + c * 16 + q, b, cplx, C, alpha, beta, bz, 1);
   };
-  bool last = tile.nsplit == 1;
+  // Pass 0 (split tiles): recombine and store this CTA's FP64 partial tile; the CTA that
+  // arrives last on the tile's counter runs pass 1 with the partials added in split order.
+  // Pass 1: final values to C. One loop body, so each step is emitted once.
   double *mine = part + (int64_t)(tile.pbase + tile.sid) * (64 * 128);  // [col][row]
+  int pass = tile.nsplit > 1 ? 0 : 1;
+  while (true) {
 #pragma unroll 1
-  for (int c = 0; c < 4; ++c) {
-    double v[16];
-    recombine(c, v);
-    if (last) {
-      final_store(c, v);
-    } else {
-#pragma unroll
-      for (int q = 0; q < 16; ++q) __stcg(&mine[(c * 16 + q) * 128 + row], v[q]);
-    }
-  }
-  if (!last) {
-    __threadfence();
-    __syncthreads();
-    if (tid == 0) *ticket = atomicAdd(&pcnt[tile.slot], 1);
-    __syncthreads();
-    if (*ticket == tile.nsplit - 1) {  // the last CTA of the tile adds the partials in split order
-      __threadfence();
-#pragma unroll 1
-      for (int c = 0; c < 4; ++c) {
-        double v[16];
+    for (int c = 0; c < 4; ++c) {
+      double v[16];
+      if (pass == 0 || tile.nsplit == 1) {
+        recombine(c, v);
+      } else {
 #pragma unroll
         for (int q = 0; q < 16; ++q) v[q] = 0.0;
 #pragma unroll 4
-        for (int sp = 0; sp < tile.nsplit; ++sp) {
+        for (int sp = 0; sp < tile.nsplit; ++sp) {  // split order: deterministic sum
           const double *src = part + (int64_t)(tile.pbase + sp) * (64 * 128);
           double t[16];
 #pragma unroll
@@ -770,10 +775,25 @@ __global__ void __launch_bounds__(128, 1)
 #pragma unroll
           for (int q = 0; q < 16; ++q) v[q] += t[q];
         }
+      }
+      if (pass == 0) {
+#pragma unroll
+        for (int q = 0; q < 16; ++q) __stcg(&mine[(c * 16 + q) * 128 + row], v[q]);
+      } else {
         final_store(c, v);
       }
-      if (tid == 0) pcnt[tile.slot] = 0;
     }
+    if (pass == 1) {
+      if (tile.nsplit > 1 && tid == 0) pcnt[tile.slot] = 0;
+      break;
+    }
+    __threadfence();
+    __syncthreads();
+    if (tid == 0) *ticket = atomicAdd(&pcnt[tile.slot], 1);
+    __syncthreads();
+    if (*ticket != tile.nsplit - 1) break;
+    __threadfence();
+    pass = 1;
   }
   tc_fence_before();
   __syncthreads();
@@ -982,7 +1002,7 @@ int launch_split(tkb_ctx *ctx, const tkb_plan *p, void *C, const void *A, const 
     k<<<grid, 256, smem, ctx->stream>>>(p->blocks, p->stiles, (int)p->nstiles, ctx->counters,
                                         (const int8_t *)ctx->ws, cplx, (double *)C, a, b);
   } else {
-    const size_t smem = ring_stages(S) * (size_t)S * (PANEL_A + PANEL_B) * KSTAGE + 512;
+    const size_t smem = ring_stages(S) * (size_t)S * (PANEL_A + PANEL_B) * KSTAGE + 1024;
     auto k = gemm_split_tc_kernel<S>;
     TKB_CUDA_TRY(ctx, cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     // programmatic dependent launch: barrier set-up and TMEM allocation overlap the slicing
