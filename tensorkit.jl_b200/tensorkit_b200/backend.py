@@ -25,7 +25,7 @@ _DEFAULT_CACHE = 10_000
 
 class _Settings(threading.local):
     def __init__(self):
-        self.precision = os.environ.get("TKB_PRECISION", "plain")   # "plain" | "split"
+        self.precision = os.environ.get("TKB_PRECISION", "plain")   # "plain" | "split" | "auto"
         self.slices = int(os.environ.get("TKB_SLICES", "0"))        # 0 = automatic
 
 
@@ -37,8 +37,8 @@ def precision():
 
 
 def set_precision(mode: str, slices: int = 0):
-    if mode not in ("plain", "split"):
-        raise ValueError("precision must be 'plain' or 'split'")
+    if mode not in ("plain", "split", "auto"):
+        raise ValueError("precision must be 'plain', 'split' or 'auto'")
     _settings.precision = mode
     _settings.slices = int(slices)
 

@@ -76,10 +76,46 @@ def gemm_plan(ctx, tC, tA, tB, prec=None, slices=None):
     def make():
         blocks = block_gemm_descriptors(tC, tA, tB)
         lens = (tA.data.numel(), tB.data.numel(), tC.data.numel())
+        if mode == "auto":
+            return _autotune(ctx, tC, tA, tB, blocks, lens, code, sl)
         return GemmPlan(ctx, blocks, lens, code,
                         L.TKB_SPLIT_INT8 if mode == "split" else L.TKB_PLAIN, sl)
 
     return ctx.plans.get_or(key, make)
+
+
+def _autotune(ctx, tC, tA, tB, blocks, lens, code, sl, reps=5):
+    """Precision "auto": build the plain FP64 and the split-precision plan of this block
+    structure, time both on the operands at hand (into a scratch output, CUDA events on the
+    library stream) and keep the faster; the choice is cached with the plan, per
+    (structure, dtype). Both forms meet the 1e-12 relative bound on the workloads."""
+    import torch
+    cands = {m: GemmPlan(ctx, blocks, lens, code, L.TKB_SPLIT_INT8 if m == "split" else L.TKB_PLAIN, sl)
+             for m in ("plain", "split")}
+    scratch = torch.empty_like(tC.data)
+    times = {}
+    _sync_in(ctx)
+    with torch.cuda.stream(ctx.stream):
+        for m, plan in cands.items():
+            def go():
+                L.check(ctx.lib.tkb_grouped_gemm(ctx.handle, plan.handle, C.c_void_p(scratch.data_ptr()),
+                                                 C.c_void_p(tA.data.data_ptr()), C.c_void_p(tB.data.data_ptr()),
+                                                 _scalar(1.0), _scalar(0.0)), ctx.handle)
+            for _ in range(2):
+                go()
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(ctx.stream)
+            for _ in range(reps):
+                go()
+            b.record(ctx.stream)
+            ctx.stream.synchronize()
+            times[m] = a.elapsed_time(b) / reps * 1e3
+    best = min(times, key=times.get)
+    for m, plan in cands.items():
+        if m != best:
+            plan.free()
+    cands[best].tuned = {"choice": best, "us": times}
+    return cands[best]
 
 
 def mul_(tC: TensorMap, tA, tB, alpha=1.0, beta=0.0, prec=None, slices=None):
