@@ -99,6 +99,8 @@ __global__ void __launch_bounds__(128)
                     const double *__restrict__ B, double alpha, double beta) {
   __shared__ __align__(16) SmemR s;
   __shared__ int next_tile;
+  pdl_wait();  // operands, output and the work-queue counters belong to earlier kernels too
+  pdl_trigger();
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int wm = warp & 1, wn = warp >> 1;
   const int g = lane >> 2, t = lane & 3;
@@ -244,6 +246,8 @@ __global__ void __launch_bounds__(256)
   extern __shared__ __align__(16) unsigned char smem_raw[];
   SmemC &s = *reinterpret_cast<SmemC *>(smem_raw);
   __shared__ int next_tile;
+  pdl_wait();
+  pdl_trigger();
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;  // 8 warps: 2 (m) x 4 (n)
   const int wm = warp & 1, wn = warp >> 1;                      // warp tile 32 x 16
   const int g = lane >> 2, t = lane & 3;
@@ -379,6 +383,8 @@ __global__ void __launch_bounds__(kSkinnyRows)
                        T *__restrict__ C, const T *__restrict__ A, const T *__restrict__ B, CDbl alpha,
                        CDbl beta) {
   __shared__ T Bs[D * D];
+  pdl_wait();
+  pdl_trigger();
   for (int64_t ti = blockIdx.x; ti < ntasks; ti += gridDim.x) {
     const GTile tk = tasks[ti];
     const GBlock b = blocks[tk.block];
@@ -444,8 +450,8 @@ int tkb_gemm_skinny_launch(tkb_ctx *ctx, const tkb_plan *p, void *C, const void 
                          gemm_skinny_kernel<double, false, 16>},
                         {gemm_skinny_kernel<double, true, 4>, gemm_skinny_kernel<double, true, 8>,
                          gemm_skinny_kernel<double, true, 16>}};
-    ks[bz][dsel]<<<grid, kSkinnyRows, 0, ctx->stream>>>(p->blocks, p->sktasks, p->nsk, (double *)C,
-                                                        (const double *)A, (const double *)B, a, bb);
+    TKB_CUDA_TRY(ctx, launch_pdl(ks[bz][dsel], dim3(grid), dim3(kSkinnyRows), 0, ctx->stream, p->blocks,
+                                 p->sktasks, p->nsk, (double *)C, (const double *)A, (const double *)B, a, bb));
   } else {
     using K = void (*)(const GBlock *, const GTile *, int64_t, double2 *, const double2 *, const double2 *, CDbl,
                        CDbl);
@@ -453,8 +459,9 @@ int tkb_gemm_skinny_launch(tkb_ctx *ctx, const tkb_plan *p, void *C, const void 
                          gemm_skinny_kernel<double2, false, 16>},
                         {gemm_skinny_kernel<double2, true, 4>, gemm_skinny_kernel<double2, true, 8>,
                          gemm_skinny_kernel<double2, true, 16>}};
-    ks[bz][dsel]<<<grid, kSkinnyRows, 0, ctx->stream>>>(p->blocks, p->sktasks, p->nsk, (double2 *)C,
-                                                        (const double2 *)A, (const double2 *)B, a, bb);
+    TKB_CUDA_TRY(ctx, launch_pdl(ks[bz][dsel], dim3(grid), dim3(kSkinnyRows), 0, ctx->stream, p->blocks,
+                                 p->sktasks, p->nsk, (double2 *)C, (const double2 *)A, (const double2 *)B, a,
+                                 bb));
   }
   ctx->launches++;
   TKB_CUDA_TRY(ctx, cudaGetLastError());
@@ -468,17 +475,17 @@ int tkb_gemm_launch(tkb_ctx *ctx, const tkb_plan *p, void *C, const void *A, con
     if (alpha.im != 0.0 || beta.im != 0.0)
       return tkb_set_error(ctx, TKB_ERR_ARG, "complex scalar with real data");
     const int grid = (int)std::min<int64_t>(p->ntiles, (int64_t)ctx->num_sms * 4);
-    gemm_f64_kernel<<<grid, 128, 0, ctx->stream>>>(p->blocks, p->tiles, (int)p->ntiles,
-                                                   ctx->counters, (double *)C, (const double *)A,
-                                                   (const double *)B, alpha.re, beta.re);
+    TKB_CUDA_TRY(ctx, launch_pdl(gemm_f64_kernel, dim3(grid), dim3(128), 0, ctx->stream, p->blocks, p->tiles,
+                                 (int)p->ntiles, ctx->counters, (double *)C, (const double *)A,
+                                 (const double *)B, alpha.re, beta.re));
   } else {
     const int grid = (int)std::min<int64_t>(p->ntiles, (int64_t)ctx->num_sms * 2);
     const size_t smem = sizeof(SmemC);
     TKB_CUDA_TRY(ctx, cudaFuncSetAttribute(gemm_c128_kernel,
                                            cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    gemm_c128_kernel<<<grid, 256, smem, ctx->stream>>>(
-        p->blocks, p->tiles, (int)p->ntiles, ctx->counters, (double2 *)C, (const double2 *)A,
-        (const double2 *)B, CDbl{alpha.re, alpha.im}, CDbl{beta.re, beta.im});
+    TKB_CUDA_TRY(ctx, launch_pdl(gemm_c128_kernel, dim3(grid), dim3(256), smem, ctx->stream, p->blocks, p->tiles,
+                                 (int)p->ntiles, ctx->counters, (double2 *)C, (const double2 *)A,
+                                 (const double2 *)B, CDbl{alpha.re, alpha.im}, CDbl{beta.re, beta.im}));
   }
   ctx->launches++;
   TKB_CUDA_TRY(ctx, cudaGetLastError());

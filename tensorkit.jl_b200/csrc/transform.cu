@@ -86,6 +86,7 @@ __global__ void __launch_bounds__(kThreads, sizeof(T) == 8 ? 3 : 2)
   const T alpha = scalar_from<T>(alpha_);
   const T beta = scalar_from<T>(beta_);
   const bool bz = beta_zero != 0;
+  pdl_wait();     // source and destination belong to earlier kernels of the stream too
   pdl_trigger();  // the next kernel may be scheduled; it waits for this grid before reading
 
   // Each CTA walks a contiguous range of tasks (tasks of one group are contiguous, so the
@@ -276,6 +277,7 @@ __global__ void __launch_bounds__(kThreads)
     for (int i = threadIdx.x; i < nw; i += kThreads) dstw[i] = __ldg(srcw + i);
   }
   __syncthreads();
+  pdl_wait();  // the records are static; source and destination belong to earlier kernels
 
   auto issue = [&](int64_t task, T *stage) {
     const TaskRec &R = rs[task - t_begin];
@@ -700,10 +702,11 @@ int tkb_transform_launch(tkb_ctx *ctx, const tkb_table *t, int dtype, void *dst,
     pg = std::max<int64_t>(pg, (t->ntasks + kRecCache - 1) / kRecCache);
     const int pgrid = (int)pg;
     if (kd)
-      kd<<<pgrid, kThreads, smem, ctx->stream>>>(t->task_rec, t->ntasks, (double *)dst, (const double *)src, a, b, bz);
+      TKB_CUDA_TRY(ctx, launch_pdl(kd, dim3(pgrid), dim3(kThreads), smem, ctx->stream, t->task_rec, t->ntasks,
+                                   (double *)dst, (const double *)src, a, b, bz));
     else
-      kc<<<pgrid, kThreads, smem, ctx->stream>>>(t->task_rec, t->ntasks, (double2 *)dst, (const double2 *)src, a, b,
-                                                 bz);
+      TKB_CUDA_TRY(ctx, launch_pdl(kc, dim3(pgrid), dim3(kThreads), smem, ctx->stream, t->task_rec, t->ntasks,
+                                   (double2 *)dst, (const double2 *)src, a, b, bz));
     ctx->launches++;
     TKB_CUDA_TRY(ctx, cudaGetLastError());
     return TKB_OK;
@@ -714,16 +717,16 @@ int tkb_transform_launch(tkb_ctx *ctx, const tkb_table *t, int dtype, void *dst,
     const size_t smem = t->smem_f64;
     auto k = treetransform_kernel<double, false>;
     if (smem > 48 * 1024) TKB_CUDA_TRY(ctx, cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    k<<<grid, kThreads, smem, ctx->stream>>>(t->groups, t->task_group, t->task_idx, t->ntasks,
-                                            t->sstr, t->soff, t->dstr, t->doff, t->coeffs,
-                                            (double *)dst, (const double *)src, a, b, bz);
+    TKB_CUDA_TRY(ctx, launch_pdl(k, dim3(grid), dim3(kThreads), smem, ctx->stream, t->groups, t->task_group,
+                                 t->task_idx, t->ntasks, t->sstr, t->soff, t->dstr, t->doff, t->coeffs,
+                                 (double *)dst, (const double *)src, a, b, bz));
   } else if (dtype == TKB_C128) {
     const size_t smem = t->smem_c128;
     auto k = conj ? treetransform_kernel<double2, true> : treetransform_kernel<double2, false>;
     if (smem > 48 * 1024) TKB_CUDA_TRY(ctx, cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    k<<<grid, kThreads, smem, ctx->stream>>>(t->groups, t->task_group, t->task_idx, t->ntasks,
-                                            t->sstr, t->soff, t->dstr, t->doff, t->coeffs,
-                                            (double2 *)dst, (const double2 *)src, a, b, bz);
+    TKB_CUDA_TRY(ctx, launch_pdl(k, dim3(grid), dim3(kThreads), smem, ctx->stream, t->groups, t->task_group,
+                                 t->task_idx, t->ntasks, t->sstr, t->soff, t->dstr, t->doff, t->coeffs,
+                                 (double2 *)dst, (const double2 *)src, a, b, bz));
   } else {
     return tkb_set_error(ctx, TKB_ERR_ARG, "unknown dtype");
   }
