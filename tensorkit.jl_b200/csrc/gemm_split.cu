@@ -3,9 +3,9 @@
 // Method (Ozaki, Ogita, Oishi & Rump 2012; Ootomo, Ozaki & Yokota 2024, "DGEMM on integer
 // matrix multiplication unit"): every row i of op(A) is scaled by 2^-e_i (e_i the binary
 // exponent bounding the row's largest magnitude) and cut into S int8 slices,
-//     A_il·2^-e_i = Σ_{s=1..S} a^(s)_il · 2^-7s + r_il,   |a^(s)| ≤ 127,  |r| < 2^-7S,
-// each slice being the truncated next 7 bits (the subtraction of the integer part is exact
-// in FP64). Columns of op(B) are cut the same way with exponents f_j. Then
+//     A_il·2^-e_i = Σ_{s=1..S} a^(s)_il · 2^-7s + r_il,   |a^(s)| ≤ 127,  |r| ≤ 2^-(7S+1),
+// the slices being the signed base-128 digits of |A_il|·2^(7S−e_i) rounded to an integer.
+// Columns of op(B) are cut the same way with exponents f_j. Then
 //     C_ij ≈ 2^(e_i+f_j) Σ_{d=2..S+1} 2^-7d P_d,ij ,   P_d = Σ_{s+t=d} a^(s) b^(t),
 // where every P_d is an exact INT32 tensor-core accumulation (K ranges of at most
 // (2^31 − 1)/(S·127²) per product task keep it exact; longer K loops are split). Terms with
@@ -180,39 +180,47 @@ __device__ __forceinline__ bool load_tile(int t, const typename SrcVal<CPLX>::T 
   }
 }
 
-// Integer slicing. For a row with exponent e (every |v| < 2^e), Y = floor(|v|·2^(7S−e)) < 2^(7S)
-// comes straight from the bits of v: v = ±m·2^(E−1075) (normal; subnormal: E = 1, no hidden
-// bit), so Y = m >> (e − 7S + 1075 − E), a right shift of at least 53 − 7S ≥ 4 bits when v is
-// normal. The S slices are the base-128 digits of Y, most significant first, each carrying
-// the sign of v: exactly the digits of S rounds of (y ← 128·y, q ← trunc(y), y ← y − q) on
-// y = v·2^−e, so the dropped low-order products keep random signs (no bias across K).
-struct Fixed {
-  uint32_t hi;  // Y >> 28
-  uint32_t lo;  // Y mod 2^28
+// Integer slicing. The row exponent e is the binary exponent of the row maximum m
+// (m = f·2^e, f in [0.5, 1)), raised by one when round(f·2^(7S)) would reach 2^(7S), so that
+// Y = round(|v|·2^(7S−e)) < 2^(7S) for every v of the row. Y is read from the mantissa of
+// z = fma(|v|·sa, sb, 2^52) with sa·sb = 2^(7S−e): both factors are normal powers of two,
+// |v|·sa is exact, the fused multiply-add rounds once, and a double in [2^52, 2^53) holds
+// z − 2^52 = Y in its low 52 bits. The S slices are the base-128 digits of Y, most
+// significant first, each carrying the sign of v, so the dropped low-order products keep
+// random signs (no bias across K).
+template <int S>
+__device__ __forceinline__ int row_exponent(double m) {
+  if (!(m > 0.0)) return 0;
+  int e;
+  const double f = frexp(m, &e);
+  return f >= 1.0 - pow2i(-(7 * S + 1)) ? e + 1 : e;
+}
+struct RowScale {
+  double sa, sb;  // sa·sb = 2^(7S−e); sa = 1 unless 2^(7S−e) is not a normal double
 };
 template <int S>
-__device__ __forceinline__ Fixed to_fixed(double v, int e, bool &neg) {
-  const uint64_t bits = (uint64_t)__double_as_longlong(v);
-  const int E = (int)((bits >> 52) & 0x7ff);
-  uint64_t m = bits & 0xfffffffffffffull;
-  int Ee = 1;
-  if (E != 0) {
-    m |= 1ull << 52;
-    Ee = E;
-  }
-  const int sh = e - 7 * S + 1075 - Ee;  // < 0 only for rows whose maximum is subnormal
-  const uint64_t y = sh >= 64 ? 0ull : sh >= 0 ? (m >> sh) : (m << -sh);
-  neg = (bits >> 63) != 0;
-  return Fixed{(uint32_t)(y >> 28), (uint32_t)y & 0xfffffffu};
+__device__ __forceinline__ RowScale row_scale(int e) {
+  const int t = 7 * S - e;  // in [7S − 1025, 7S + 1073]
+  const int b = t <= 1000 ? t : 1000;
+  return RowScale{pow2i(t - b), pow2i(b)};
 }
-// byte masks of the negative values among 16 (0xff per negative value, 4 words)
-__device__ __forceinline__ void sign_masks(const bool (&neg)[16], uint32_t (&M)[4]) {
+struct Fixed {
+  uint32_t hi;  // bits 32..63 of z (Y >> 32 in the low bits)
+  uint32_t lo;  // Y mod 2^32
+};
+__device__ __forceinline__ Fixed to_fixed(double v, const RowScale &rs) {
+  const double z = fma(fabs(v) * rs.sa, rs.sb, 4503599627370496.0);  // 2^52 + Y
+  return Fixed{(uint32_t)__double2hiint(z), (uint32_t)__double2loint(z)};
+}
+// byte masks of the negative values among 16 (0xff per value with its sign bit set, 4 words)
+template <typename F>
+__device__ __forceinline__ void sign_masks(F &&val, uint32_t (&M)[4]) {
 #pragma unroll
   for (int h = 0; h < 4; ++h) {
-    uint32_t m = 0u;
+    uint32_t s[4];
 #pragma unroll
-    for (int b = 0; b < 4; ++b) m |= (neg[4 * h + b] ? 0xffu : 0u) << (8 * b);
-    M[h] = m;
+    for (int b = 0; b < 4; ++b) s[b] = (uint32_t)(__double2hiint(val(4 * h + b)) >> 31);
+    M[h] = __byte_perm(__byte_perm(s[0], s[1], 0x0040), __byte_perm(s[2], s[3], 0x0040), 0x5410);
   }
 }
 // digit sl (0 = most significant) of 16 fixed-point values as one 16-byte chunk of int8:
@@ -222,12 +230,12 @@ template <int S>
 __device__ __forceinline__ uint4 slice16(const Fixed (&x)[16], const uint32_t (&M)[4], int sl) {
   const int sh = 7 * (S - 1 - sl);
   uint32_t d[16];
-  if (sh >= 28) {
+  if (sh >= 32) {
 #pragma unroll
-    for (int q = 0; q < 16; ++q) d[q] = x[q].hi >> (sh - 28);
+    for (int q = 0; q < 16; ++q) d[q] = x[q].hi >> (sh - 32);
   } else {
 #pragma unroll
-    for (int q = 0; q < 16; ++q) d[q] = (x[q].lo >> sh) | (x[q].hi << (28 - sh));
+    for (int q = 0; q < 16; ++q) d[q] = __funnelshift_r(x[q].lo, x[q].hi, sh);
   }
   uint32_t w[4];
 #pragma unroll
@@ -316,9 +324,7 @@ __device__ __forceinline__ void slice_task(const GBlock &b, int op, int64_t r0, 
     unsigned long long mb = rmax[tid];
     for (uint32_t q = 0; q < csize; ++q)
       if (q != crank) mb = max(mb, ld_dsmem_u64(&rmax[tid], q));
-    const double m = __longlong_as_double((long long)mb);
-    int e = 0;
-    if (m > 0.0) frexp(m, &e);
+    const int e = row_exponent<S>(__longlong_as_double((long long)mb));
     rexp[tid] = e;
     int32_t *ex = reinterpret_cast<int32_t *>(ws + (op == 0 ? b.wsEA : b.wsEB));
     const int64_t r = r0 + tid;
@@ -347,31 +353,29 @@ __device__ __forceinline__ void slice_task(const GBlock &b, int op, int64_t r0, 
     int64_t c;
     const bool ok = load_tile<CPLX, ROWC>(t, X, xo, rs, ks, r0, msrc, b.k, kfull, stage, lane, v, row, c);
     if (!ok) continue;
-    const int e = rexp[row];
+    const RowScale rsc = row_scale<S>(rexp[row]);
     const int64_t r = r0 + row;
     // one slice per iteration (not unrolled: the body is reused S times, which keeps the
     // code of this short-lived kernel small)
     if constexpr (!CPLX) {
       Fixed x[16];
-      bool ng[16];
       uint32_t M[4];
 #pragma unroll
-      for (int q = 0; q < 16; ++q) x[q] = to_fixed<S>(v[q], e, ng[q]);
-      sign_masks(ng, M);
+      for (int q = 0; q < 16; ++q) x[q] = to_fixed(v[q], rsc);
+      sign_masks([&](int q) { return v[q]; }, M);
       int8_t *p = base + slice_off(r, c, kpad, pr);
 #pragma unroll 1
       for (int sl = 0; sl < S; ++sl, p += plane) *reinterpret_cast<uint4 *>(p) = slice16<S>(x, M, sl);
     } else {
       Fixed xr[16], xi[16];
-      bool nr[16], ni[16];
       uint32_t Mr[4], Mi[4], Mn[4];
 #pragma unroll
       for (int q = 0; q < 16; ++q) {
-        xr[q] = to_fixed<S>(v[q].x, e, nr[q]);
-        xi[q] = to_fixed<S>(conj ? -v[q].y : v[q].y, e, ni[q]);
+        xr[q] = to_fixed(v[q].x, rsc);
+        xi[q] = to_fixed(v[q].y, rsc);
       }
-      sign_masks(nr, Mr);
-      sign_masks(ni, Mi);
+      sign_masks([&](int q) { return v[q].x; }, Mr);
+      sign_masks([&](int q) { return conj ? -v[q].y : v[q].y; }, Mi);
       if (op == 0) {  // rows 2r: [Re | -Im], 2r+1: [Im | Re]
 #pragma unroll
         for (int h = 0; h < 4; ++h) Mn[h] = ~Mi[h];
