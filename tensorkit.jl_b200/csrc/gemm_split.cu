@@ -30,7 +30,7 @@
 //   is split across CTAs); one thread streams the S slice stages of A and B with
 //   cp.async.bulk into a shared-memory ring as deep as fits (5 stages at S = 7) and issues
 //   tcgen05.mma.kind::i8 (M=128, N=64, K=32) into S int32 accumulators held in tensor memory (S·64 of 512
-//   columns); four warps read the accumulators back with tcgen05.ld and recombine them in
+//   columns); eight warps (two per TMEM lane quarter) read the accumulators back with tcgen05.ld and recombine them in
 //   FP64.
 //   mma.sync kernel (TKB_SPLIT_KERNEL=mma): the same products with int8 mma.sync.
 #include <algorithm>
@@ -545,17 +545,37 @@ constexpr uint32_t kIdescI8 = (2u << 4) | (1u << 7) | (1u << 10) | ((64u >> 3) <
 
 // One product task: output tile (m0, n0) of a block, K stages [kb, ke). When a tile's K
 // range is split over nsplit CTAs (few tiles, long K), each CTA recombines its own int32
-// diagonals into an FP64 partial tile and stores it (plain coalesced stores) in partial
-// buffer pbase + sid; the CTA that arrives last on the tile's counter adds the partials in
-// split order (deterministic), scales, writes C and resets the counter for the next launch.
+// diagonals into an FP64 partial tile, and the partials are added in split order
+// (deterministic) before the scaling and the store to C:
+//   CL = true: the pieces of a tile are the CTAs of one thread-block cluster; each keeps its
+//     partial in its own (now idle) ring memory, and after a cluster barrier CTA `sid` reduces
+//     the column chunks sid, sid + nsplit, … of the tile through distributed shared memory.
+//     Clusters without a split tile hold up to cluster-size independent tiles (or idle CTAs,
+//     kind 2).
+//   CL = false: each piece stores its partial (plain coalesced stores) in partial buffer
+//     pbase + sid; the CTA that arrives last on the tile's counter adds the partials, writes C
+//     and resets the counter for the next launch (any number of pieces).
 struct SplitTile {
   int32_t block, m0, n0, kind;
   int32_t kb, ke, slot, nsplit;
   int32_t sid, pbase;
 };
 
-template <int S>
-__global__ void __launch_bounds__(128, 1)
+__device__ __forceinline__ uint32_t mapa_u32(uint32_t saddr, uint32_t rank) {
+  uint32_t r;
+  asm volatile("mapa.shared::cluster.u32 %0, %1, %2;\n" : "=r"(r) : "r"(saddr), "r"(rank));
+  return r;
+}
+__device__ __forceinline__ double ld_dsmem_f64(uint32_t addr) {
+  double v;
+  asm volatile("ld.shared::cluster.f64 %0, [%1];\n" : "=d"(v) : "r"(addr) : "memory");
+  return v;
+}
+
+constexpr int kTcThreads = 256;
+
+template <int S, bool CL>
+__global__ void __launch_bounds__(kTcThreads, 1)
     gemm_split_tc_kernel(const GBlock *__restrict__ blocks, const SplitTile *__restrict__ tiles,
                          const int8_t *__restrict__ ws, int cplx, double *__restrict__ C, CDbl alpha,
                          CDbl beta, int *err, double *__restrict__ part, int *__restrict__ pcnt) {
@@ -574,6 +594,7 @@ __global__ void __launch_bounds__(128, 1)
   const SplitTile tile = tiles[blockIdx.x];
   const GBlock b = blocks[tile.block];
   const bool has_k = tile.kind == 0;
+  const bool idle = CL && tile.kind == 2;  // padding CTA of a cluster
   const int kb = tile.kb;
   const int nk = has_k ? tile.ke - tile.kb : 0;
   const bool bz = beta.x == 0.0 && beta.y == 0.0;
@@ -597,7 +618,7 @@ __global__ void __launch_bounds__(128, 1)
   tc_fence_after();
   const uint32_t tmem = has_k ? *tmem_slot : 0u;
   pdl_wait();  // slices and exponents come from the slicing kernel (set-up above overlapped it)
-  if (tid >= 64) {  // column exponents into shared memory while warp 0 starts the products
+  if (tid >= 64 && tid < 128) {  // column exponents into shared memory while warp 0 starts the products
     const int col = tid - 64;
     const int64_t j = tile.n0 + col;
     const int ej = (has_k && j < b.n) ? max(reinterpret_cast<const int32_t *>(ws + b.wsEB)[j], -1100) : 0;
@@ -677,10 +698,12 @@ __global__ void __launch_bounds__(128, 1)
   }
   __syncwarp();  // tcgen05.ld is warp-collective: reconverge after the divergent waits
   __syncthreads();  // ebs visible; every warp is past its wait
-  // epilogue: warp w owns accumulator rows 32w..32w+31 (TMEM lanes)
+  // epilogue: warp w owns accumulator rows 32(w mod 4) .. 32(w mod 4) + 31 (the TMEM lanes its
+  // warp may read) and the column chunks 2·half, 2·half + 1 (16 columns each), half = w / 4
   const int32_t *eA = reinterpret_cast<const int32_t *>(ws + b.wsEA);
   const int64_t Mreal = cplx ? 2 * b.m : b.m;
-  const int row = 32 * warp + lane;
+  const int row = 32 * (warp & 3) + lane;
+  const int half = warp >> 2;
   const int64_t i = tile.m0 + row;
   const int ei = (has_k && i < Mreal) ? max(eA[i], -1100) : 0;
   const double rscale = (ei >= -1022 && ei <= 1023) ? pow2i(ei) : 0.0;
@@ -693,7 +716,7 @@ __global__ void __launch_bounds__(128, 1)
     uint32_t r[S][16];
 #pragma unroll
     for (int d = 0; d < S; ++d)
-      tmem_ld16_issue(tmem + ((uint32_t)(32 * warp) << 16) + (uint32_t)(d * 64 + c * 16), r[d]);
+      tmem_ld16_issue(tmem + ((uint32_t)(32 * (warp & 3)) << 16) + (uint32_t)(d * 64 + c * 16), r[d]);
 #pragma unroll
     for (int d = 0; d < S; ++d) tmem_ld_wait(r[d]);
     // exact integer recombination: diagonals d = 0..2, 3..4, 5..6 are combined by Horner's
@@ -756,6 +779,50 @@ __global__ void __launch_bounds__(128, 1)
 #pragma unroll
     for (int q = 0; q < 16; ++q) store_out(v[q], i, tile.n0 + c * 16 + q, b, cplx, C, alpha, beta, bz, 1);
   };
+  if constexpr (CL) {
+    // the ring is idle (every stage landed and every product completed): it holds this CTA's
+    // FP64 partial tile, [column][row]
+    double *P = reinterpret_cast<double *>(smem);
+    const bool split = tile.nsplit > 1;
+    if (!idle) {
+      if (split) asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+#pragma unroll 1
+      for (int c = 2 * half; c < 2 * half + 2; ++c) {
+        double v[16];
+        recombine(c, v);
+        if (split) {
+#pragma unroll
+          for (int q = 0; q < 16; ++q) P[(c * 16 + q) * 128 + row] = v[q];
+        } else {
+          final_store(c, v);
+        }
+      }
+    }
+    cluster_arrive();
+    cluster_wait();
+    if (split) {
+      const uint32_t pb = smem_u32(P) + (uint32_t)row * 8u;
+#pragma unroll 1
+      for (int c = tile.sid + half * tile.nsplit; c < 4; c += 2 * tile.nsplit) {
+        double v[16];
+#pragma unroll
+        for (int q = 0; q < 16; ++q) v[q] = 0.0;
+#pragma unroll 1
+        for (int sp = 0; sp < tile.nsplit; ++sp) {  // split order: deterministic sum
+          const uint32_t rb = mapa_u32(pb, (uint32_t)sp) + (uint32_t)(c * 16 * 128 * 8);
+          double t[16];
+#pragma unroll
+          for (int q = 0; q < 16; ++q) t[q] = ld_dsmem_f64(rb + (uint32_t)(q * 128 * 8));
+#pragma unroll
+          for (int q = 0; q < 16; ++q) v[q] += t[q];
+        }
+        final_store(c, v);
+      }
+    }
+    // no CTA leaves while a peer may still read its partial
+    cluster_arrive();
+    cluster_wait();
+  } else {
   // Pass 0 (split tiles): recombine and store this CTA's FP64 partial tile; the CTA that
   // arrives last on the tile's counter runs pass 1 with the partials added in split order.
   // Pass 1: final values to C. One loop body, so each step is emitted once.
@@ -763,7 +830,7 @@ __global__ void __launch_bounds__(128, 1)
   int pass = tile.nsplit > 1 ? 0 : 1;
   while (true) {
 #pragma unroll 1
-    for (int c = 0; c < 4; ++c) {
+    for (int c = 2 * half; c < 2 * half + 2; ++c) {
       double v[16];
       if (pass == 0 || tile.nsplit == 1) {
         recombine(c, v);
@@ -798,6 +865,7 @@ __global__ void __launch_bounds__(128, 1)
     if (*ticket != tile.nsplit - 1) break;
     __threadfence();
     pass = 1;
+  }
   }
   tc_fence_before();
   __syncthreads();
@@ -960,6 +1028,8 @@ __global__ void __launch_bounds__(256)
   }
 }
 
+size_t tc_smem_bytes(int S) { return ring_stages(S) * (size_t)S * (PANEL_A + PANEL_B) * KSTAGE + 1024; }
+
 bool use_mma_sync() {
   const char *e = std::getenv("TKB_SPLIT_KERNEL");
   return e && std::strcmp(e, "mma") == 0;
@@ -1006,20 +1076,30 @@ int launch_split(tkb_ctx *ctx, const tkb_plan *p, void *C, const void *A, const 
     k<<<grid, 256, smem, ctx->stream>>>(p->blocks, p->stiles, (int)p->nstiles, ctx->counters,
                                         (const int8_t *)ctx->ws, cplx, (double *)C, a, b);
   } else {
-    const size_t smem = ring_stages(S) * (size_t)S * (PANEL_A + PANEL_B) * KSTAGE + 1024;
-    auto k = gemm_split_tc_kernel<S>;
+    const size_t smem = tc_smem_bytes(S);
+    const bool cl = p->kcluster > 1;
+    auto k = cl ? gemm_split_tc_kernel<S, true> : gemm_split_tc_kernel<S, false>;
     TKB_CUDA_TRY(ctx, cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     // programmatic dependent launch: barrier set-up and TMEM allocation overlap the slicing
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3((unsigned)p->nkstiles);
-    cfg.blockDim = dim3(128);
+    cfg.blockDim = dim3(kTcThreads);
     cfg.dynamicSmemBytes = smem;
     cfg.stream = ctx->stream;
-    cudaLaunchAttribute attr[1];
-    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
-    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cudaLaunchAttribute attr[2];
+    int na = 0;
+    if (p->nsrows > 0) {
+      attr[na].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+      attr[na++].val.programmaticStreamSerializationAllowed = 1;
+    }
+    if (cl) {
+      attr[na].id = cudaLaunchAttributeClusterDimension;
+      attr[na].val.clusterDim.x = (unsigned)p->kcluster;
+      attr[na].val.clusterDim.y = 1;
+      attr[na++].val.clusterDim.z = 1;
+    }
     cfg.attrs = attr;
-    cfg.numAttrs = p->nsrows > 0 ? 1 : 0;
+    cfg.numAttrs = na;
     TKB_CUDA_TRY(ctx, cudaLaunchKernelEx(&cfg, k, (const GBlock *)p->blocks, (const SplitTile *)p->kstiles,
                                          (const int8_t *)ctx->ws, cplx, (double *)C, a, b, ctx->counters + 8,
                                          p->part, p->pcnt));
@@ -1030,6 +1110,78 @@ int launch_split(tkb_ctx *ctx, const tkb_plan *p, void *C, const void *A, const 
 }
 
 int64_t roundup(int64_t x, int64_t m) { return (x + m - 1) / m * m; }
+
+// Co-resident thread-block clusters of `cs` product CTAs (one CTA per SM; clusters stay within
+// one GPC, so this is below num_sms / cs on parts whose GPCs have SM counts not divisible by cs).
+template <int S>
+int max_clusters_t(int cs, cudaStream_t st) {
+  auto k = gemm_split_tc_kernel<S, true>;
+  const size_t smem = tc_smem_bytes(S);
+  if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) return 0;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3((unsigned)cs);
+  cfg.blockDim = dim3(kTcThreads);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = st;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = (unsigned)cs;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  int n = 0;
+  if (cudaOccupancyMaxActiveClusters(&n, k, &cfg) != cudaSuccess) {
+    cudaGetLastError();
+    return 0;
+  }
+  return n;
+}
+int max_clusters(int S, int cs, cudaStream_t st) {
+  switch (S) {
+    case 3: return max_clusters_t<3>(cs, st);
+    case 4: return max_clusters_t<4>(cs, st);
+    case 5: return max_clusters_t<5>(cs, st);
+    case 6: return max_clusters_t<6>(cs, st);
+    default: return max_clusters_t<7>(cs, st);
+  }
+}
+
+// Cluster split plan: tiles with more than T stages are cut into cs pieces (one cluster each),
+// the others are grouped cs per cluster in order of decreasing K (padded with idle CTAs).
+// Cost model (tenths of a K stage of about 1.1 us, from the measured epilogues): a K stage 10,
+// the epilogue of an unsplit tile 30, of a cluster-reduced piece 48, of a global-memory-reduced
+// piece 63 + 6 per piece beyond two.
+constexpr int64_t kCostStage = 10, kCostEpi = 30, kCostEpiCluster = 48, kCostEpiGlobal = 63, kCostEpiGlobalPiece = 6;
+struct ClusterPlan {
+  int cs = 0;
+  int64_t T = 0, cost = INT64_MAX, ctas = 0;
+};
+ClusterPlan plan_clusters(const std::vector<int64_t> &nks, int S, int64_t maxst, int64_t nsm, cudaStream_t st) {
+  ClusterPlan best;
+  const int64_t nt = (int64_t)nks.size();  // stages per tile, decreasing (0: no products)
+  for (int cs = 2; cs <= 4; ++cs) {
+    const int64_t cap = std::min<int64_t>(max_clusters(S, cs, st), nsm / cs);
+    if (cap <= 0) continue;
+    // candidate thresholds: split the first ns tiles (those with the most stages)
+    for (int64_t ns = 1; ns <= nt; ++ns) {
+      if (nks[ns - 1] < 2 * cs) break;  // every piece keeps at least two stages
+      const int64_t clusters = ns + (nt - ns + cs - 1) / cs;
+      if (clusters > cap) continue;
+      const int64_t piece = (nks[0] + cs - 1) / cs;
+      const int64_t rest = ns < nt ? nks[ns] : 0;
+      if (piece > maxst || rest > maxst) continue;
+      const int64_t cost = std::max(piece * kCostStage + kCostEpiCluster, rest * kCostStage + kCostEpi);
+      if (cost < best.cost || (cost == best.cost && clusters * cs < best.ctas)) {
+        best.cs = cs;
+        best.T = rest;
+        best.cost = cost;
+        best.ctas = clusters * cs;
+      }
+    }
+  }
+  return best;
+}
 
 }  // namespace
 
@@ -1102,6 +1254,12 @@ int tkb_gemm_split_prepare(tkb_ctx *ctx, tkb_plan *p) {
     auto pieces = [&](int64_t nk, int64_t target) {
       return (int)std::max<int64_t>(std::min<int64_t>(8, (nk + target - 1) / target), (nk + maxst - 1) / maxst);
     };
+    // cluster plan (partials reduced through distributed shared memory) when it beats both
+    // the unsplit plan and the global-memory split plan below
+    std::vector<int64_t> nks;
+    for (const GTile &t : tiles) nks.push_back(t.kind == 0 ? p->hblocks[t.block].kpad / KSTAGE : 0);
+    ClusterPlan cp;
+    if (nt < nsm && std::getenv("TKB_SPLIT_REDUCE") == nullptr) cp = plan_clusters(nks, S, maxst, nsm, ctx->stream);
     int64_t target = maxnk;  // no split
     if (nt < nsm) {
       target = std::max<int64_t>(4, (total + nsm - 1) / nsm);
@@ -1111,7 +1269,52 @@ int tkb_gemm_split_prepare(tkb_ctx *ctx, tkb_plan *p) {
         if (cnt <= nsm) break;
       }
     }
+    // the global-memory split plan's cost in the same model
+    int64_t gcost = 0;
     for (const GTile &t : tiles) {
+      const int64_t nk = t.kind == 0 ? p->hblocks[t.block].kpad / KSTAGE : 0;
+      const int ks = t.kind == 0 ? pieces(nk, target) : 1;
+      gcost = std::max<int64_t>(gcost, (nk + ks - 1) / ks * kCostStage +
+                                           (ks > 1 ? kCostEpiGlobal + kCostEpiGlobalPiece * (ks - 2) : kCostEpi));
+    }
+    const bool use_cl = cp.cs > 1 && cp.cost < gcost;
+    p->kcluster = use_cl ? cp.cs : 0;
+    if (use_cl) {
+      // tiles are sorted by decreasing K: split the leading ones, group the rest
+      const int cs = cp.cs;
+      struct Cl {
+        int64_t len;
+        SplitTile t[4];
+      };
+      std::vector<Cl> cls;
+      size_t i = 0;
+      for (; i < tiles.size() && nks[i] > cp.T; ++i) {
+        const GTile &t = tiles[i];
+        const int nk = (int)nks[i];
+        Cl c;
+        c.len = (nk + cs - 1) / cs;
+        for (int s = 0; s < cs; ++s) c.t[s] = {t.block, t.m0, t.n0, 0, s * nk / cs, (s + 1) * nk / cs, -1, cs, s, 0};
+        cls.push_back(c);
+      }
+      while (i < tiles.size()) {
+        Cl c;
+        c.len = nks[i];
+        for (int s = 0; s < cs; ++s, ++i) {
+          if (i < tiles.size()) {
+            const GTile &t = tiles[i];
+            c.t[s] = {t.block, t.m0, t.n0, t.kind, 0, (int)nks[i], -1, 1, s, 0};
+          } else {
+            c.t[s] = {0, 0, 0, 2, 0, 0, -1, 1, s, 0};  // idle
+          }
+        }
+        cls.push_back(c);
+      }
+      std::stable_sort(cls.begin(), cls.end(), [](const Cl &x, const Cl &y) { return x.len > y.len; });
+      for (const Cl &c : cls)
+        for (int s = 0; s < cs; ++s) kt.push_back(c.t[s]);
+    }
+    for (const GTile &t : tiles) {
+      if (use_cl) break;
       const int nk = p->hblocks[t.block].kpad / KSTAGE;
       const int ks = t.kind == 0 ? pieces(nk, target) : 1;
       if (ks == 1) {
@@ -1123,9 +1326,10 @@ int tkb_gemm_split_prepare(tkb_ctx *ctx, tkb_plan *p) {
         npart += ks;
       }
     }
-    std::stable_sort(kt.begin(), kt.end(), [](const SplitTile &x, const SplitTile &y) {
-      return (x.ke - x.kb) > (y.ke - y.kb);
-    });
+    if (!use_cl)
+      std::stable_sort(kt.begin(), kt.end(), [](const SplitTile &x, const SplitTile &y) {
+        return (x.ke - x.kb) > (y.ke - y.kb);
+      });
   }
   p->ws_bytes = off;
   p->nstiles = (int64_t)tiles.size();

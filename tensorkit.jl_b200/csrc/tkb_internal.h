@@ -191,6 +191,7 @@ struct tkb_plan {
   int64_t nkstiles = 0;
   double *part = nullptr;       // split-K FP64 partial tiles (rewritten every launch)
   int *pcnt = nullptr;          // split-K arrival counters (self-clearing)
+  int kcluster = 0;             // > 1: split tiles reduced inside clusters of this many CTAs
   void *sjobs = nullptr;        // slice jobs (block, operand)
   int64_t *srow_begin = nullptr;
   int nsjobs = 0;

@@ -75,3 +75,26 @@ def test_split_error_decreases_with_slices(slices):
     err = relerr(C.to_host(), ref.data)
     # truncation bound of the slicing: ~2^-7S per operand, times a modest k-dependent factor
     assert err <= 2.0 ** (-7 * slices) * 64
+
+
+@pytest.mark.parametrize("cplx", [False, True])
+def test_split_k_reductions(cplx, monkeypatch):
+    """Few output tiles with long K: the K loops are split over several CTAs, whose partial
+    tiles are reduced inside thread-block clusters (default) or through global memory
+    (TKB_SPLIT_REDUCE set); both meet the split-precision tolerance, with α and β."""
+    A, B = _mats(cplx, mult=8)
+    ref = O.mul(A, B)
+    C0 = O.randn(ref.W, 4, cplx)
+    Ad, Bd = to_device(A), to_device(B)
+    ctx = tk.get_context(Ad.device.index)
+    want = 0.5 * ref.data - 2.0 * C0.data
+    for mode in (None, "global"):
+        if mode is None:
+            monkeypatch.delenv("TKB_SPLIT_REDUCE", raising=False)
+        else:
+            monkeypatch.setenv("TKB_SPLIT_REDUCE", mode)
+        ctx.empty_caches()
+        Cd = to_device(C0)
+        tk.mul_(Cd, Ad, Bd, 0.5, -2.0, prec="split")
+        assert relerr(Cd.to_host(), want) <= TOL_SPLIT
+    ctx.empty_caches()
