@@ -83,31 +83,48 @@ __host__ __device__ __forceinline__ int64_t slice_off(int64_t r, int64_t kb, int
 }
 
 // Slicing pass: one task = 32 source rows of one operand of one block over the whole K range,
-// run by a thread-block cluster of 1, 2 or 4 CTAs that split the K range (the partial row
-// maxima are combined through distributed shared memory). Source rows are the rows of op(A)
+// run by g of the kSliceCluster CTAs of a thread-block cluster (g sized so that every warp has
+// about one warp tile, tasks packed into clusters by the host), which split the K range (the
+// partial row maxima are combined through distributed shared memory). Source rows are the rows of op(A)
 // and the columns of op(B) (for ComplexF64 a complex source row of op(A) gives the real row
 // pair 2r, 2r+1). The cluster first reduces the row maxima (phase 1), derives the row
-// exponents, then re-reads the rows (now cached) and writes the S slices (phase 2) as 16-byte
-// chunks of 16 consecutive K of one row in the tensor-core operand layout.
+// exponents, then re-reads the rows (now cached) and writes the S slices (phase 2) as 8-byte
+// pieces (8 consecutive K of one row) of the tensor-core operand layout.
 //
-// Every warp works on warp tiles; after loading, each lane holds 16 consecutive K values of
-// one source row:
+// Every warp works on warp tiles; after loading, each lane holds LK consecutive K values of
+// one source row, LK = 8 (small tiles: many warps per task and short per-warp chains, for
+// slicing passes that fit one wave) or 16 (fewer instructions per value, for larger ones):
 //   rows contiguous in memory (real op(A) = A, op(B) = Bᵀ; complex likewise): lane = row,
-//     tile = 32 rows × 16 K, loads straight from global memory (coalesced along rows);
+//     tile = 32 rows × LK K, loads straight from global memory (coalesced along rows);
 //   K contiguous (op(A) = Aᵀ/Aᴴ, op(B) = B): lanes along K (coalesced), staged through a
-//     per-warp shared-memory tile (one padding element per 16) and read back row-wise:
-//     real 4 rows × 128 K, complex 8 rows × 64 K.
-// ComplexF64 K is laid out as [Re | Im] halves of kh = round_up(k, 16) positions each, so a
-// 16-K chunk of the source maps to one chunk in each half.
-struct SliceTask {
+//     per-warp shared-memory tile (one padding element per LK) and read back row-wise:
+//     real 4 rows × 8·LK K, complex 8 rows × 4·LK K.
+// ComplexF64 K is laid out as [Re | Im] halves of kh = round_up(k, 16) positions each, so an
+// LK piece of the source maps to one piece in each half.
+struct SliceTask {  // one entry per CTA
   int32_t block;
-  int32_t operand;  // 0 = rows of op(A), 1 = columns of op(B)
+  int32_t operand;  // 0 = rows of op(A), 1 = columns of op(B), -1 = idle CTA
   int32_t r0;       // first source row
-  int32_t kfull;    // padded source K (real: kpad; complex: kpad / 2), for ordering
+  int32_t sub;      // index of this CTA among the task's CTAs
+  int32_t g;        // number of CTAs of the task
+  int32_t rank0;    // cluster rank of the task's first CTA
 };
 
 constexpr int kSliceThreads = 256;
-constexpr int kSliceWarpSmem = 8 * 68 * 16;  // bytes of one warp's staging tile (complex; real: half)
+constexpr int kSliceCluster = 4;  // CTAs per thread-block cluster of the slicing pass
+// bytes of one warp's staging tile (complex: 8 rows × 4·LK K of 16-byte values, one padding
+// value per LK; real: half)
+__host__ __device__ constexpr int slice_warp_smem(int LK) { return 8 * 4 * (LK + 1) * 16; }
+template <int LK>
+struct Piece;  // LK int8 digits: one store per slice
+template <>
+struct Piece<8> {
+  using T = uint2;
+};
+template <>
+struct Piece<16> {
+  using T = uint4;
+};
 
 template <bool CPLX>
 struct SrcVal;
@@ -125,30 +142,30 @@ __device__ __forceinline__ double2 zero_of(double2) { return make_double2(0.0, 0
 __device__ __forceinline__ double absmax(double v) { return fabs(v); }
 __device__ __forceinline__ double absmax(double2 v) { return fmax(fabs(v.x), fabs(v.y)); }
 
-// Loads warp tile t into v[16]; returns the lane's source row (relative to the task) and the
-// source K of v[0] through row/c; false when the lane's chunk lies beyond the padded K.
-template <bool CPLX, bool ROWC>
+// Loads warp tile t into v[LK]; returns the lane's source row (relative to the task) and the
+// source K of v[0] through row/c; false when the lane's piece lies beyond the padded K.
+template <bool CPLX, bool ROWC, int LK>
 __device__ __forceinline__ bool load_tile(int t, const typename SrcVal<CPLX>::T *__restrict__ X,
                                           int64_t xo, int64_t rs, int64_t ks, int64_t r0,
                                           int64_t msrc, int64_t ksrc, int64_t kfull,
                                           typename SrcVal<CPLX>::T *stage, int lane,
-                                          typename SrcVal<CPLX>::T (&v)[16], int &row, int64_t &c) {
+                                          typename SrcVal<CPLX>::T (&v)[LK], int &row, int64_t &c) {
   using T = typename SrcVal<CPLX>::T;
   const T z = zero_of(T{});
   if constexpr (ROWC) {
     row = lane;
-    c = 16 * (int64_t)t;
+    c = LK * (int64_t)t;
     const int64_t r = r0 + lane;
     const bool rv = r < msrc;
     const T *p = X + xo + r * rs;
 #pragma unroll
-    for (int q = 0; q < 16; ++q) v[q] = (rv && c + q < ksrc) ? __ldg(p + (c + q) * ks) : z;
+    for (int q = 0; q < LK; ++q) v[q] = (rv && c + q < ksrc) ? __ldg(p + (c + q) * ks) : z;
     return true;
   } else {
     constexpr int RG = CPLX ? 8 : 4;       // rows per warp tile
-    constexpr int KW = CPLX ? 64 : 128;    // K per warp tile
+    constexpr int KW = (CPLX ? 4 : 8) * LK;  // K per warp tile
     constexpr int NH = KW / 32;            // loads per row per lane
-    constexpr int RP = (KW / 16) * 17;     // staging row pitch (elements)
+    constexpr int RP = (KW / LK) * (LK + 1);  // staging row pitch (elements)
     const int ngrp = 32 / RG;
     const int grp = t % ngrp;
     const int64_t k0 = (int64_t)(t / ngrp) * KW;
@@ -168,14 +185,16 @@ __device__ __forceinline__ bool load_tile(int t, const typename SrcVal<CPLX>::T 
 #pragma unroll
     for (int rr = 0; rr < RG; ++rr)
 #pragma unroll
-      for (int h = 0; h < NH; ++h) stage[rr * RP + (2 * h + (lane >> 4)) * 17 + (lane & 15)] = tmp[rr * NH + h];
+      for (int h = 0; h < NH; ++h)
+        stage[rr * RP + ((32 / LK) * h + lane / LK) * (LK + 1) + lane % LK] = tmp[rr * NH + h];
     __syncwarp();
     constexpr int LPR = 32 / RG;  // lanes per row
+    static_assert(LPR * LK == KW, "one warp tile row is read back by LPR lanes");
     const int rr = lane / LPR, kap = lane % LPR;
 #pragma unroll
-    for (int q = 0; q < 16; ++q) v[q] = stage[rr * RP + kap * 17 + q];
+    for (int q = 0; q < LK; ++q) v[q] = stage[rr * RP + kap * (LK + 1) + q];
     row = grp * RG + rr;
-    c = k0 + 16 * kap;
+    c = k0 + LK * kap;
     return c < kfull;
   }
 }
@@ -212,51 +231,48 @@ __device__ __forceinline__ Fixed to_fixed(double v, const RowScale &rs) {
   const double z = fma(fabs(v) * rs.sa, rs.sb, 4503599627370496.0);  // 2^52 + Y
   return Fixed{(uint32_t)__double2hiint(z), (uint32_t)__double2loint(z)};
 }
-// byte masks of the negative values among 16 (0xff per value with its sign bit set, 4 words)
-template <typename F>
-__device__ __forceinline__ void sign_masks(F &&val, uint32_t (&M)[4]) {
+// byte masks of the negative values among 4·NW (0xff per value with its sign bit set)
+template <int NW, typename F>
+__device__ __forceinline__ void sign_masks(F &&val, uint32_t (&M)[NW]) {
 #pragma unroll
-  for (int h = 0; h < 4; ++h) {
+  for (int h = 0; h < NW; ++h) {
     uint32_t s[4];
 #pragma unroll
     for (int b = 0; b < 4; ++b) s[b] = (uint32_t)(__double2hiint(val(4 * h + b)) >> 31);
     M[h] = __byte_perm(__byte_perm(s[0], s[1], 0x0040), __byte_perm(s[2], s[3], 0x0040), 0x5410);
   }
 }
-// digit sl (0 = most significant) of 16 fixed-point values as one 16-byte chunk of int8:
+// digit sl (0 = most significant) of LK fixed-point values as one LK-byte piece of int8:
 // the 7-bit digit of Y, negated in the bytes that M marks (bytes 0..127: the negation is
 // (0x80 − b) ^ 0x80, with no carry between bytes)
-template <int S>
-__device__ __forceinline__ uint4 slice16(const Fixed (&x)[16], const uint32_t (&M)[4], int sl) {
+template <int S, int LK>
+__device__ __forceinline__ typename Piece<LK>::T slice_piece(const Fixed (&x)[LK], const uint32_t (&M)[LK / 4],
+                                                             int sl) {
   const int sh = 7 * (S - 1 - sl);
-  uint32_t d[16];
+  uint32_t d[LK];
   if (sh >= 32) {
 #pragma unroll
-    for (int q = 0; q < 16; ++q) d[q] = x[q].hi >> (sh - 32);
+    for (int q = 0; q < LK; ++q) d[q] = x[q].hi >> (sh - 32);
   } else {
 #pragma unroll
-    for (int q = 0; q < 16; ++q) d[q] = __funnelshift_r(x[q].lo, x[q].hi, sh);
+    for (int q = 0; q < LK; ++q) d[q] = __funnelshift_r(x[q].lo, x[q].hi, sh);
   }
-  uint32_t w[4];
+  uint32_t w[LK / 4];
 #pragma unroll
-  for (int h = 0; h < 4; ++h) {
+  for (int h = 0; h < LK / 4; ++h) {
     const uint32_t u = __byte_perm(__byte_perm(d[4 * h], d[4 * h + 1], 0x0040),
                                    __byte_perm(d[4 * h + 2], d[4 * h + 3], 0x0040), 0x5410) & 0x7f7f7f7fu;
     const uint32_t n = (0x80808080u - u) ^ 0x80808080u;
     w[h] = (u & ~M[h]) | (n & M[h]);
   }
-  return make_uint4(w[0], w[1], w[2], w[3]);
+  if constexpr (LK == 8) return make_uint2(w[0], w[1]);
+  else return make_uint4(w[0], w[1], w[2], w[3]);
 }
 
 // thread-block cluster helpers (the K range of a task is split over the CTAs of a cluster)
 __device__ __forceinline__ uint32_t cluster_rank() {
   uint32_t r;
   asm volatile("mov.u32 %0, %%cluster_ctarank;\n" : "=r"(r));
-  return r;
-}
-__device__ __forceinline__ uint32_t cluster_size() {
-  uint32_t r;
-  asm volatile("mov.u32 %0, %%cluster_nctarank;\n" : "=r"(r));
   return r;
 }
 __device__ __forceinline__ void cluster_arrive() {
@@ -277,17 +293,19 @@ __device__ __forceinline__ unsigned long long ld_dsmem_u64(const void *p, uint32
   return v;
 }
 
-template <int S, bool CPLX, bool ROWC>
-__device__ __forceinline__ void slice_task(const GBlock &b, int op, int64_t r0, const void *Xv, int8_t *ws,
+template <int S, bool CPLX, bool ROWC, int LK>
+__device__ __forceinline__ void slice_task(const GBlock &b, const SliceTask &task, const void *Xv, int8_t *ws,
                                            unsigned char *wsmem, unsigned long long *rmax, int *rexp) {
   using T = typename SrcVal<CPLX>::T;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  // the CTAs of a cluster share the task's warp tiles: crank·8 + warp, then every 8·csize
-  const uint32_t crank = cluster_rank(), csize = cluster_size();
-  const int t0 = (int)crank * (kSliceThreads / 32) + warp;
-  const int tstep = (int)csize * (kSliceThreads / 32);
+  const int op = task.operand;
+  const int64_t r0 = task.r0;
+  // the task's CTAs share its warp tiles: sub·8 + warp, then every 8·g
+  const uint32_t crank = cluster_rank();
+  const int t0 = task.sub * (kSliceThreads / 32) + warp;
+  const int tstep = task.g * (kSliceThreads / 32);
   const T *X = reinterpret_cast<const T *>(Xv);
-  T *stage = reinterpret_cast<T *>(wsmem + warp * (CPLX ? kSliceWarpSmem : kSliceWarpSmem / 2));
+  T *stage = reinterpret_cast<T *>(wsmem + warp * (CPLX ? slice_warp_smem(LK) : slice_warp_smem(LK) / 2));
   const int64_t xo = op == 0 ? b.offA : b.offB;
   const int opx = op == 0 ? b.opA : b.opB;
   // strides of source rows and K in elements
@@ -302,33 +320,33 @@ __device__ __forceinline__ void slice_task(const GBlock &b, int op, int64_t r0, 
   const bool conj = opx == TKB_OP_C;
   const int64_t msrc = op == 0 ? b.m : b.n;
   const int64_t kfull = CPLX ? b.kpad / 2 : b.kpad;
-  const int ntile = ROWC ? (int)(kfull / 16)
-                         : (CPLX ? 4 : 8) * (int)((kfull + (CPLX ? 63 : 127)) / (CPLX ? 64 : 128));
+  const int ntile = ROWC ? (int)(kfull / LK)
+                         : (CPLX ? 4 : 8) * (int)((kfull + (CPLX ? 4 : 8) * LK - 1) / ((CPLX ? 4 : 8) * LK));
 
   // phase 1: row maxima of this CTA's tiles
   for (int t = t0; t < ntile; t += tstep) {
-    T v[16];
+    T v[LK];
     int row;
     int64_t c;
-    load_tile<CPLX, ROWC>(t, X, xo, rs, ks, r0, msrc, b.k, kfull, stage, lane, v, row, c);
+    load_tile<CPLX, ROWC, LK>(t, X, xo, rs, ks, r0, msrc, b.k, kfull, stage, lane, v, row, c);
     double m = 0.0;
 #pragma unroll
-    for (int q = 0; q < 16; ++q) m = fmax(m, absmax(v[q]));
+    for (int q = 0; q < LK; ++q) m = fmax(m, absmax(v[q]));
     if (m > 0.0) atomicMax(&rmax[row], (unsigned long long)__double_as_longlong(m));
   }
-  // partial maxima of the cluster's CTAs → row exponents (written by CTA 0)
+  // partial maxima of the task's CTAs → row exponents (written by the task's first CTA)
   __syncthreads();
   cluster_arrive();
   cluster_wait();
   if (tid < 32) {
     unsigned long long mb = rmax[tid];
-    for (uint32_t q = 0; q < csize; ++q)
+    for (uint32_t q = (uint32_t)task.rank0; q < (uint32_t)(task.rank0 + task.g); ++q)
       if (q != crank) mb = max(mb, ld_dsmem_u64(&rmax[tid], q));
     const int e = row_exponent<S>(__longlong_as_double((long long)mb));
     rexp[tid] = e;
     int32_t *ex = reinterpret_cast<int32_t *>(ws + (op == 0 ? b.wsEA : b.wsEB));
     const int64_t r = r0 + tid;
-    if (crank == 0) {
+    if (task.sub == 0) {
       if (CPLX && op == 0) {
         ex[2 * r] = e;
         ex[2 * r + 1] = e;
@@ -348,29 +366,31 @@ __device__ __forceinline__ void slice_task(const GBlock &b, int op, int64_t r0, 
   int8_t *base = ws + (op == 0 ? b.wsA : b.wsB);
   const int64_t plane = (int64_t)(op == 0 ? b.mpad : b.npad) * kpad;
   for (int t = t0; t < ntile; t += tstep) {
-    T v[16];
+    T v[LK];
     int row;
     int64_t c;
-    const bool ok = load_tile<CPLX, ROWC>(t, X, xo, rs, ks, r0, msrc, b.k, kfull, stage, lane, v, row, c);
+    const bool ok = load_tile<CPLX, ROWC, LK>(t, X, xo, rs, ks, r0, msrc, b.k, kfull, stage, lane, v, row, c);
     if (!ok) continue;
     const RowScale rsc = row_scale<S>(rexp[row]);
     const int64_t r = r0 + row;
     // one slice per iteration (not unrolled: the body is reused S times, which keeps the
     // code of this short-lived kernel small)
     if constexpr (!CPLX) {
-      Fixed x[16];
-      uint32_t M[4];
+      using P = typename Piece<LK>::T;
+      Fixed x[LK];
+      uint32_t M[LK / 4];
 #pragma unroll
-      for (int q = 0; q < 16; ++q) x[q] = to_fixed(v[q], rsc);
+      for (int q = 0; q < LK; ++q) x[q] = to_fixed(v[q], rsc);
       sign_masks([&](int q) { return v[q]; }, M);
       int8_t *p = base + slice_off(r, c, kpad, pr);
 #pragma unroll 1
-      for (int sl = 0; sl < S; ++sl, p += plane) *reinterpret_cast<uint4 *>(p) = slice16<S>(x, M, sl);
+      for (int sl = 0; sl < S; ++sl, p += plane) *reinterpret_cast<P *>(p) = slice_piece<S, LK>(x, M, sl);
     } else {
-      Fixed xr[16], xi[16];
-      uint32_t Mr[4], Mi[4], Mn[4];
+      using P = typename Piece<LK>::T;
+      Fixed xr[LK], xi[LK];
+      uint32_t Mr[LK / 4], Mi[LK / 4], Mn[LK / 4];
 #pragma unroll
-      for (int q = 0; q < 16; ++q) {
+      for (int q = 0; q < LK; ++q) {
         xr[q] = to_fixed(v[q].x, rsc);
         xi[q] = to_fixed(v[q].y, rsc);
       }
@@ -378,19 +398,19 @@ __device__ __forceinline__ void slice_task(const GBlock &b, int op, int64_t r0, 
       sign_masks([&](int q) { return conj ? -v[q].y : v[q].y; }, Mi);
       if (op == 0) {  // rows 2r: [Re | -Im], 2r+1: [Im | Re]
 #pragma unroll
-        for (int h = 0; h < 4; ++h) Mn[h] = ~Mi[h];
+        for (int h = 0; h < LK / 4; ++h) Mn[h] = ~Mi[h];
         int8_t *p0 = base + slice_off(2 * r, c, kpad, pr);
         int8_t *p1 = base + slice_off(2 * r, kfull + c, kpad, pr);
         int8_t *p2 = base + slice_off(2 * r + 1, c, kpad, pr);
         int8_t *p3 = base + slice_off(2 * r + 1, kfull + c, kpad, pr);
 #pragma unroll 1
         for (int sl = 0; sl < S; ++sl) {
-          const uint4 ur = slice16<S>(xr, Mr, sl);
+          const P ur = slice_piece<S, LK>(xr, Mr, sl);
           const int64_t o = sl * plane;
-          *reinterpret_cast<uint4 *>(p0 + o) = ur;
-          *reinterpret_cast<uint4 *>(p1 + o) = slice16<S>(xi, Mn, sl);
-          *reinterpret_cast<uint4 *>(p2 + o) = slice16<S>(xi, Mi, sl);
-          *reinterpret_cast<uint4 *>(p3 + o) = ur;
+          *reinterpret_cast<P *>(p0 + o) = ur;
+          *reinterpret_cast<P *>(p1 + o) = slice_piece<S, LK>(xi, Mn, sl);
+          *reinterpret_cast<P *>(p2 + o) = slice_piece<S, LK>(xi, Mi, sl);
+          *reinterpret_cast<P *>(p3 + o) = ur;
         }
       } else {        // column j of op(B): [Re | Im]
         int8_t *p0 = base + slice_off(r, c, kpad, pr);
@@ -398,8 +418,8 @@ __device__ __forceinline__ void slice_task(const GBlock &b, int op, int64_t r0, 
 #pragma unroll 1
         for (int sl = 0; sl < S; ++sl) {
           const int64_t o = sl * plane;
-          *reinterpret_cast<uint4 *>(p0 + o) = slice16<S>(xr, Mr, sl);
-          *reinterpret_cast<uint4 *>(p1 + o) = slice16<S>(xi, Mi, sl);
+          *reinterpret_cast<P *>(p0 + o) = slice_piece<S, LK>(xr, Mr, sl);
+          *reinterpret_cast<P *>(p1 + o) = slice_piece<S, LK>(xi, Mi, sl);
         }
       }
     }
@@ -407,8 +427,8 @@ __device__ __forceinline__ void slice_task(const GBlock &b, int op, int64_t r0, 
   cluster_wait();
 }
 
-template <int S, bool CPLX>
-__global__ void __launch_bounds__(kSliceThreads, CPLX ? 1 : 2)
+template <int S, bool CPLX, int LK>
+__global__ void __launch_bounds__(kSliceThreads, LK == 8 ? (CPLX ? 2 : 3) : (CPLX ? 1 : 2))
     slice_kernel(const GBlock *__restrict__ blocks, const SliceTask *__restrict__ tasks,
                  const double *__restrict__ A, const double *__restrict__ B, int8_t *ws) {
   extern __shared__ __align__(16) unsigned char slice_smem[];
@@ -416,16 +436,23 @@ __global__ void __launch_bounds__(kSliceThreads, CPLX ? 1 : 2)
   __shared__ int rexp[32];
   pdl_wait();     // the operands come from the previous kernel of the stream
   pdl_trigger();  // the product kernel may be scheduled (it waits for this grid to finish)
-  const SliceTask task = tasks[blockIdx.x / cluster_size()];
-  const GBlock &b = blocks[task.block];
+  const SliceTask task = tasks[blockIdx.x];
   const int op = task.operand;
+  if (op < 0) {  // idle CTA: the cluster barriers of the task CTAs (two phases) still count it
+    cluster_arrive();
+    cluster_wait();
+    cluster_arrive();
+    cluster_wait();
+    return;
+  }
+  const GBlock &b = blocks[task.block];
   if (threadIdx.x < 32) rmax[threadIdx.x] = 0ull;
   __syncthreads();
   const int opx = op == 0 ? b.opA : b.opB;
   const bool rowc = op == 0 ? opx == TKB_OP_N : opx != TKB_OP_N;
   const void *X = op == 0 ? (const void *)A : (const void *)B;
-  if (rowc) slice_task<S, CPLX, true>(b, op, task.r0, X, ws, slice_smem, rmax, rexp);
-  else slice_task<S, CPLX, false>(b, op, task.r0, X, ws, slice_smem, rmax, rexp);
+  if (rowc) slice_task<S, CPLX, true, LK>(b, task, X, ws, slice_smem, rmax, rexp);
+  else slice_task<S, CPLX, false, LK>(b, task, X, ws, slice_smem, rmax, rexp);
 }
 
 // ---- shared epilogue: recombine one output value --------------------------------------------
@@ -1040,20 +1067,19 @@ int launch_split(tkb_ctx *ctx, const tkb_plan *p, void *C, const void *A, const 
   const int cplx = p->dtype == TKB_C128 ? 1 : 0;
   if (p->nsrows > 0) {
     // complex tiles stage 16-byte elements: twice the shared memory of real ones
-    const size_t smem = (size_t)(kSliceThreads / 32) * kSliceWarpSmem / (cplx ? 1 : 2);
-    auto k = cplx ? slice_kernel<S, true> : slice_kernel<S, false>;
+    const int lk = p->slice_lk;
+    const size_t smem = (size_t)(kSliceThreads / 32) * slice_warp_smem(lk) / (cplx ? 1 : 2);
+    auto k = lk == 8 ? (cplx ? slice_kernel<S, true, 8> : slice_kernel<S, false, 8>)
+                     : (cplx ? slice_kernel<S, true, 16> : slice_kernel<S, false, 16>);
     TKB_CUDA_TRY(ctx, cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    // CTAs per task (a thread-block cluster): as many as still fit one wave at two CTAs per SM
-    int cs = 1;
-    while (cs < 4 && p->nsrows * (cs * 2) <= 2 * (int64_t)ctx->num_sms) cs *= 2;
     cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = dim3((unsigned)(p->nsrows * cs));
+    cfg.gridDim = dim3((unsigned)p->nsrows);
     cfg.blockDim = dim3(kSliceThreads);
     cfg.dynamicSmemBytes = smem;
     cfg.stream = ctx->stream;
     cudaLaunchAttribute attr[2];
     attr[0].id = cudaLaunchAttributeClusterDimension;
-    attr[0].val.clusterDim.x = cs;
+    attr[0].val.clusterDim.x = kSliceCluster;
     attr[0].val.clusterDim.y = 1;
     attr[0].val.clusterDim.z = 1;
     attr[1].id = cudaLaunchAttributeProgrammaticStreamSerialization;
@@ -1110,6 +1136,48 @@ int launch_split(tkb_ctx *ctx, const tkb_plan *p, void *C, const void *A, const 
 }
 
 int64_t roundup(int64_t x, int64_t m) { return (x + m - 1) / m * m; }
+
+// Co-resident clusters of the slicing pass (kSliceCluster CTAs each)
+template <int S, bool CPLX, int LK>
+int max_slice_clusters_t(cudaStream_t st) {
+  auto k = slice_kernel<S, CPLX, LK>;
+  const size_t smem = (size_t)(kSliceThreads / 32) * slice_warp_smem(LK) / (CPLX ? 1 : 2);
+  if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) return 0;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3((unsigned)kSliceCluster);
+  cfg.blockDim = dim3(kSliceThreads);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = st;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = kSliceCluster;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  int n = 0;
+  if (cudaOccupancyMaxActiveClusters(&n, k, &cfg) != cudaSuccess) {
+    cudaGetLastError();
+    return 0;
+  }
+  return n;
+}
+template <int S>
+int max_slice_clusters_s(bool cplx, int lk, cudaStream_t st) {
+  if (lk == 8) return cplx ? max_slice_clusters_t<S, true, 8>(st) : max_slice_clusters_t<S, false, 8>(st);
+  return cplx ? max_slice_clusters_t<S, true, 16>(st) : max_slice_clusters_t<S, false, 16>(st);
+}
+int max_slice_clusters(int S, bool cplx, int lk, cudaStream_t st, int num_sms) {
+  int n = 0;
+  switch (S) {
+    case 3: n = max_slice_clusters_s<3>(cplx, lk, st); break;
+    case 4: n = max_slice_clusters_s<4>(cplx, lk, st); break;
+    case 5: n = max_slice_clusters_s<5>(cplx, lk, st); break;
+    case 6: n = max_slice_clusters_s<6>(cplx, lk, st); break;
+    default: n = max_slice_clusters_s<7>(cplx, lk, st); break;
+  }
+  return n > 0 ? n : num_sms / kSliceCluster;
+}
 
 // Co-resident thread-block clusters of `cs` product CTAs (one CTA per SM; clusters stay within
 // one GPC, so this is below num_sms / cs on parts whose GPCs have SM counts not divisible by cs).
@@ -1192,7 +1260,10 @@ int tkb_gemm_split_prepare(tkb_ctx *ctx, tkb_plan *p) {
   if (S < 3 || S > SMAX) return tkb_set_error(ctx, TKB_ERR_UNSUPPORTED, "slices must be in 3..7");
   p->slices = S;
   size_t off = 0;
-  std::vector<SliceTask> jobs;
+  struct SJob {
+    int32_t block, op, r0, kfull, rowc;
+  };
+  std::vector<SJob> sj;
   std::vector<GTile> tiles;
   for (size_t bi = 0; bi < p->hblocks.size(); ++bi) {
     GBlock &b = p->hblocks[bi];
@@ -1212,14 +1283,66 @@ int tkb_gemm_split_prepare(tkb_ctx *ctx, tkb_plan *p) {
     if (kind == 0) {
       const int32_t kfull = cplx ? b.kpad / 2 : b.kpad;
       const int32_t rows_a = cplx ? b.mpad / 2 : b.mpad;  // source rows (complex: row pairs)
-      for (int32_t r0 = 0; r0 < rows_a; r0 += 32) jobs.push_back({(int32_t)bi, 0, r0, kfull});
-      for (int32_t r0 = 0; r0 < b.npad; r0 += 32) jobs.push_back({(int32_t)bi, 1, r0, kfull});
+      const int32_t ra = b.opA == TKB_OP_N ? 1 : 0, rb = b.opB != TKB_OP_N ? 1 : 0;
+      for (int32_t r0 = 0; r0 < rows_a; r0 += 32) sj.push_back({(int32_t)bi, 0, r0, kfull, ra});
+      for (int32_t r0 = 0; r0 < b.npad; r0 += 32) sj.push_back({(int32_t)bi, 1, r0, kfull, rb});
     }
     for (int64_t m0 = 0; m0 < M; m0 += PANEL_A)
       for (int64_t n0 = 0; n0 < b.n; n0 += PANEL_B) tiles.push_back({(int32_t)bi, (int32_t)m0, (int32_t)n0, kind});
   }
-  // slicing tasks: longest K first
-  std::stable_sort(jobs.begin(), jobs.end(), [](const SliceTask &x, const SliceTask &y) { return x.kfull > y.kfull; });
+  // slicing tasks → CTAs: task j gets g_j = min(kSliceCluster, ceil(ntile_j / (8·R))) CTAs (about
+  // R warp tiles per warp), tasks are packed first-fit by decreasing g into clusters of
+  // kSliceCluster CTAs (the rest idle), and R is the smallest round count whose clusters are
+  // all co-resident. 8-K warp tiles when at most two rounds fit one wave, else 16-K tiles.
+  std::vector<SliceTask> jobs;
+  p->slice_lk = 16;
+  if (!sj.empty()) {
+    std::stable_sort(sj.begin(), sj.end(), [](const SJob &x, const SJob &y) { return x.kfull > y.kfull; });
+    const int wpc = kSliceThreads / 32;
+    auto ntile = [&](const SJob &t, int lk) -> int64_t {
+      return t.rowc ? t.kfull / lk : (cplx ? 4 : 8) * ((t.kfull + (cplx ? 4 : 8) * lk - 1) / ((cplx ? 4 : 8) * lk));
+    };
+    // packs with lk and R; false when the clusters exceed cap and `force` is not set
+    auto pack = [&](int lk, int R, int64_t cap, bool force) {
+      struct Bin {
+        int used = 0;
+        int64_t len = 0;
+        std::vector<std::pair<int, int>> items;  // (job, g)
+      };
+      std::vector<Bin> bins;
+      for (int j = 0; j < (int)sj.size(); ++j) {
+        const int64_t nt = ntile(sj[j], lk);
+        const int g = (int)std::min<int64_t>(kSliceCluster, std::max<int64_t>(1, (nt + wpc * R - 1) / (wpc * R)));
+        size_t bi = 0;
+        while (bi < bins.size() && bins[bi].used + g > kSliceCluster) ++bi;
+        if (bi == bins.size()) bins.emplace_back();
+        bins[bi].items.push_back({j, g});
+        bins[bi].used += g;
+        bins[bi].len = std::max<int64_t>(bins[bi].len, (nt + wpc * g - 1) / (wpc * g));
+      }
+      if ((int64_t)bins.size() > cap && !force) return false;
+      std::stable_sort(bins.begin(), bins.end(), [](const Bin &x, const Bin &y) { return x.len > y.len; });
+      jobs.clear();
+      for (const Bin &bn : bins) {
+        int rank = 0;
+        for (const auto &it : bn.items) {
+          const SJob &t = sj[it.first];
+          for (int q = 0; q < it.second; ++q) jobs.push_back({t.block, t.op, t.r0, q, it.second, rank});
+          rank += it.second;
+        }
+        for (; rank < kSliceCluster; ++rank) jobs.push_back({0, -1, 0, 0, 1, rank});
+      }
+      return true;
+    };
+    const int64_t cap8 = std::max<int64_t>(1, max_slice_clusters(S, cplx, 8, ctx->stream, ctx->num_sms));
+    if (pack(8, 1, cap8, false) || pack(8, 2, cap8, false)) {
+      p->slice_lk = 8;
+    } else {
+      const int64_t cap16 = std::max<int64_t>(1, max_slice_clusters(S, cplx, 16, ctx->stream, ctx->num_sms));
+      for (int R = 1;; ++R)
+        if (pack(16, R, cap16, R >= 64)) break;
+    }
+  }
   // exponent arrays of every block in one contiguous region (rewritten by every slicing pass)
   p->expo_off = (int64_t)off;
   for (size_t bi = 0; bi < p->hblocks.size(); ++bi) {
