@@ -17,12 +17,14 @@
 // [Re B; Im B], so rows 2r and 2r+1 of the real result are Re and Im of C_r. The two K
 // halves are each zero-padded to round_up(k, 16) positions.
 //
-// Slice layout in the workspace: per block, per slice, the rows of op(A) (op(B)ᵀ) are cut
-// into panels of 128 (64) rows; a panel is a sequence of 32-byte K stages (one tensor-core
-// K step), each stored as the canonical K-major "core matrix" layout of the tensor-core
-// operand descriptors (8-row × 16-byte core matrices; 256 bytes between 8-row groups, 128
-// bytes between the two 16-byte K chunks). One stage of one slice is therefore one
-// contiguous 4 KiB (2 KiB) block that a single bulk copy moves into shared memory.
+// Slice layout in the workspace: per block, the rows of op(A) (op(B)ᵀ) are cut into panels
+// of 128 (64) rows; a panel is a sequence of 32-byte K stages (one tensor-core K step), and a
+// stage holds the S slices one after another, each in the canonical K-major "core matrix"
+// layout of the tensor-core operand descriptors (8-row × 16-byte core matrices; 256 bytes
+// between 8-row groups, 128 bytes between the two 16-byte K chunks). One stage of all S
+// slices of a panel is therefore one contiguous S·4 KiB (S·2 KiB) block that a single bulk
+// copy moves into shared memory (the issue rate of one producer thread, not the copy size,
+// limits the ring).
 //
 // Launches: slicing pass (one thread-block cluster per 32 source rows: row maxima,
 // exponents, slices) + product pass:
@@ -73,13 +75,14 @@ __device__ __forceinline__ double i2d_small(int64_t x) {
   return __longlong_as_double(x + 0x4338000000000000ll) - 6755399441055744.0;
 }
 
-// byte offset of (row r, K byte kb) inside one slice plane (pr: rows per panel, 64 or 128)
-__host__ __device__ __forceinline__ int64_t slice_off(int64_t r, int64_t kb, int64_t kpad, int pr) {
+// byte offset of (slice 0, row r, K byte kb) in a block's slices (pr: rows per panel, 64 or
+// 128); slice s is s·pr·KSTAGE bytes further
+__host__ __device__ __forceinline__ int64_t slice_off(int64_t r, int64_t kb, int64_t kpad, int pr, int S) {
   const int lpr = pr == 128 ? 7 : 6;
   const int64_t panel = r >> lpr, rr = r & (pr - 1);
   const int64_t stg = kb >> 5, kk = kb & 31;
-  return panel * (pr * kpad) + stg * (pr * KSTAGE) + (rr >> 3) * 256 + (kk >> 4) * 128 +
-         (rr & 7) * 16 + (kk & 15);
+  return (panel * kpad + stg * KSTAGE) * (int64_t)(S * pr) + (rr >> 3) * 256 + (kk >> 4) * 128 + (rr & 7) * 16 +
+         (kk & 15);
 }
 
 // Slicing pass: one task = 32 source rows of one operand of one block over the whole K range,
@@ -364,7 +367,7 @@ __device__ __forceinline__ void slice_task(const GBlock &b, const SliceTask &tas
   const int pr = op == 0 ? PANEL_A : PANEL_B;
   const int64_t kpad = b.kpad;
   int8_t *base = ws + (op == 0 ? b.wsA : b.wsB);
-  const int64_t plane = (int64_t)(op == 0 ? b.mpad : b.npad) * kpad;
+  const int64_t plane = (int64_t)pr * KSTAGE;  // between the slices of one stage
   for (int t = t0; t < ntile; t += tstep) {
     T v[LK];
     int row;
@@ -382,7 +385,7 @@ __device__ __forceinline__ void slice_task(const GBlock &b, const SliceTask &tas
 #pragma unroll
       for (int q = 0; q < LK; ++q) x[q] = to_fixed(v[q], rsc);
       sign_masks([&](int q) { return v[q]; }, M);
-      int8_t *p = base + slice_off(r, c, kpad, pr);
+      int8_t *p = base + slice_off(r, c, kpad, pr, S);
 #pragma unroll 1
       for (int sl = 0; sl < S; ++sl, p += plane) *reinterpret_cast<P *>(p) = slice_piece<S, LK>(x, M, sl);
     } else {
@@ -399,10 +402,10 @@ __device__ __forceinline__ void slice_task(const GBlock &b, const SliceTask &tas
       if (op == 0) {  // rows 2r: [Re | -Im], 2r+1: [Im | Re]
 #pragma unroll
         for (int h = 0; h < LK / 4; ++h) Mn[h] = ~Mi[h];
-        int8_t *p0 = base + slice_off(2 * r, c, kpad, pr);
-        int8_t *p1 = base + slice_off(2 * r, kfull + c, kpad, pr);
-        int8_t *p2 = base + slice_off(2 * r + 1, c, kpad, pr);
-        int8_t *p3 = base + slice_off(2 * r + 1, kfull + c, kpad, pr);
+        int8_t *p0 = base + slice_off(2 * r, c, kpad, pr, S);
+        int8_t *p1 = base + slice_off(2 * r, kfull + c, kpad, pr, S);
+        int8_t *p2 = base + slice_off(2 * r + 1, c, kpad, pr, S);
+        int8_t *p3 = base + slice_off(2 * r + 1, kfull + c, kpad, pr, S);
 #pragma unroll 1
         for (int sl = 0; sl < S; ++sl) {
           const P ur = slice_piece<S, LK>(xr, Mr, sl);
@@ -413,8 +416,8 @@ __device__ __forceinline__ void slice_task(const GBlock &b, const SliceTask &tas
           *reinterpret_cast<P *>(p3 + o) = ur;
         }
       } else {        // column j of op(B): [Re | Im]
-        int8_t *p0 = base + slice_off(r, c, kpad, pr);
-        int8_t *p1 = base + slice_off(r, kfull + c, kpad, pr);
+        int8_t *p0 = base + slice_off(r, c, kpad, pr, S);
+        int8_t *p1 = base + slice_off(r, kfull + c, kpad, pr, S);
 #pragma unroll 1
         for (int sl = 0; sl < S; ++sl) {
           const int64_t o = sl * plane;
@@ -656,21 +659,14 @@ __global__ void __launch_bounds__(kTcThreads, 1)
   // producer: lane 0 of warp 0; the other lanes of warp 0 wait at the __syncwarp below (no
   // polling that would take issue slots from the producer)
   if (has_k && tid == 0) {
-    const int8_t *gA = ws + b.wsA + (int64_t)(tile.m0 / PANEL_A) * PANEL_A * b.kpad;
-    const int8_t *gB = ws + b.wsB + (int64_t)(tile.n0 / PANEL_B) * PANEL_B * b.kpad;
-    const int64_t planeA = (int64_t)b.mpad * b.kpad, planeB = (int64_t)b.npad * b.kpad;
+    const int8_t *gA = ws + b.wsA + (int64_t)(tile.m0 / PANEL_A) * S * PANEL_A * b.kpad;
+    const int8_t *gB = ws + b.wsB + (int64_t)(tile.n0 / PANEL_B) * S * PANEL_B * b.kpad;
     auto load = [&](int kt, int st) {  // kt: local stage index, global stage kb + kt
       unsigned char *sa = smem + st * STAGE;
       const int64_t kg = kb + kt;
       mbar_expect_tx(&full[st], STAGE);
-#pragma unroll
-      for (int s = 0; s < S; ++s)
-        bulk_g2s(sa + s * (PANEL_A * KSTAGE), gA + s * planeA + kg * PANEL_A * KSTAGE,
-                 PANEL_A * KSTAGE, &full[st]);
-#pragma unroll
-      for (int s = 0; s < S; ++s)
-        bulk_g2s(sa + A_BYTES + s * (PANEL_B * KSTAGE), gB + s * planeB + kg * PANEL_B * KSTAGE,
-                 PANEL_B * KSTAGE, &full[st]);
+      bulk_g2s(sa, gA + kg * A_BYTES, A_BYTES, &full[st]);
+      bulk_g2s(sa + A_BYTES, gB + kg * B_BYTES, B_BYTES, &full[st]);
     };
     // NSTAGE-deep ring: stage kt lives in slot kt % NSTAGE; its n-th use has parity n & 1.
     // After issuing the products of stage kt, the slot of stage kt-1 is refilled with stage
@@ -925,17 +921,16 @@ __device__ __forceinline__ void imma(int (&c)[4], const int (&a)[4], const int (
 template <int S>
 __device__ __forceinline__ void load_stage(int8_t *As, int8_t *Bs, const GBlock &b, const int8_t *ws,
                                            int64_t m0, int64_t n0, int64_t k0) {
-  const int64_t planeA = (int64_t)b.mpad * b.kpad, planeB = (int64_t)b.npad * b.kpad;
   for (int c = threadIdx.x; c < 2 * S * 128; c += blockDim.x) {
     const int op = c / (S * 128);
     const int rem = c % (S * 128);
     const int s = rem / 128, q = rem % 128;
     const int row = q >> 1, half = q & 1;
     if (op == 0) {
-      const int8_t *g = ws + b.wsA + s * planeA + slice_off(m0 + row, k0 + half * 16, b.kpad, PANEL_A);
+      const int8_t *g = ws + b.wsA + s * (PANEL_A * KSTAGE) + slice_off(m0 + row, k0 + half * 16, b.kpad, PANEL_A, S);
       cp_async16(As + (s * SBM + row) * SPITCH + half * 16, g);
     } else {
-      const int8_t *g = ws + b.wsB + s * planeB + slice_off(n0 + row, k0 + half * 16, b.kpad, PANEL_B);
+      const int8_t *g = ws + b.wsB + s * (PANEL_B * KSTAGE) + slice_off(n0 + row, k0 + half * 16, b.kpad, PANEL_B, S);
       cp_async16(Bs + (s * SBN + row) * SPITCH + half * 16, g);
     }
   }
