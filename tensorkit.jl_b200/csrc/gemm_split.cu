@@ -326,12 +326,27 @@ __device__ __forceinline__ void slice_task(const GBlock &b, const SliceTask &tas
   const int ntile = ROWC ? (int)(kfull / LK)
                          : (CPLX ? 4 : 8) * (int)((kfull + (CPLX ? 4 : 8) * LK - 1) / ((CPLX ? 4 : 8) * LK));
 
-  // phase 1: row maxima of this CTA's tiles
+  // phase 1: row maxima of this CTA's tiles. With 8-K real tiles the warp's first tile stays
+  // in registers for phase 2 (most warps have one tile).
+  constexpr bool KEEP = LK == 8 && !CPLX;
+  T keep[KEEP ? LK : 1];
+  int krow = 0;
+  int64_t kc = 0;
+  bool kok = false;
   for (int t = t0; t < ntile; t += tstep) {
     T v[LK];
     int row;
     int64_t c;
-    load_tile<CPLX, ROWC, LK>(t, X, xo, rs, ks, r0, msrc, b.k, kfull, stage, lane, v, row, c);
+    const bool ok = load_tile<CPLX, ROWC, LK>(t, X, xo, rs, ks, r0, msrc, b.k, kfull, stage, lane, v, row, c);
+    if constexpr (KEEP) {
+      if (t == t0) {
+#pragma unroll
+        for (int q = 0; q < LK; ++q) keep[q] = v[q];
+        krow = row;
+        kc = c;
+        kok = ok;
+      }
+    }
     double m = 0.0;
 #pragma unroll
     for (int q = 0; q < LK; ++q) m = fmax(m, absmax(v[q]));
@@ -358,9 +373,9 @@ __device__ __forceinline__ void slice_task(const GBlock &b, const SliceTask &tas
       }
     }
   }
-  // done reading the peers' maxima; the matching wait before exit keeps every CTA's shared
-  // memory alive until all peers have read it
-  cluster_arrive();
+  // done reading the peers' maxima (no ordering needed: relaxed); the matching wait before exit
+  // keeps every CTA's shared memory alive until all peers have read it
+  asm volatile("barrier.cluster.arrive.relaxed.aligned;\n" ::: "memory");
   __syncthreads();
 
   // phase 2: slices
@@ -372,7 +387,16 @@ __device__ __forceinline__ void slice_task(const GBlock &b, const SliceTask &tas
     T v[LK];
     int row;
     int64_t c;
-    const bool ok = load_tile<CPLX, ROWC, LK>(t, X, xo, rs, ks, r0, msrc, b.k, kfull, stage, lane, v, row, c);
+    bool ok;
+    if (KEEP && t == t0) {
+#pragma unroll
+      for (int q = 0; q < LK; ++q) v[q] = keep[KEEP ? q : 0];
+      row = krow;
+      c = kc;
+      ok = kok;
+    } else {
+      ok = load_tile<CPLX, ROWC, LK>(t, X, xo, rs, ks, r0, msrc, b.k, kfull, stage, lane, v, row, c);
+    }
     if (!ok) continue;
     const RowScale rsc = row_scale<S>(rexp[row]);
     const int64_t r = r0 + row;
