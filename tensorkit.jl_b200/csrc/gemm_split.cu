@@ -542,6 +542,17 @@ __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity) {
     if (globaltimer_ns() - t0 > 2000000000ull) return false;
   }
 }
+// bounded wait until *p ≥ target (acquire at GPU scope); false once 2 s have passed
+__device__ __forceinline__ bool wait_count(const int *p, int target) {
+  const uint64_t t0 = globaltimer_ns();
+  while (true) {
+    int v;
+    asm volatile("ld.acquire.gpu.global.s32 %0, [%1];\n" : "=r"(v) : "l"(p) : "memory");
+    if (v >= target) return true;
+    if (globaltimer_ns() - t0 > 2000000000ull) return false;
+    __nanosleep(32);
+  }
+}
 __device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t bytes, uint64_t *bar) {
   asm volatile(
       "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(
@@ -607,8 +618,9 @@ constexpr uint32_t kIdescI8 = (2u << 4) | (1u << 7) | (1u << 10) | ((64u >> 3) <
 //     Clusters without a split tile hold up to cluster-size independent tiles (or idle CTAs,
 //     kind 2).
 //   CL = false: each piece stores its partial (plain coalesced stores) in partial buffer
-//     pbase + sid; the CTA that arrives last on the tile's counter adds the partials, writes C
-//     and resets the counter for the next launch (any number of pieces).
+//     pbase + sid; when the launch is one wave, every piece waits for the others and reduces a
+//     share of the column chunks, otherwise the CTA that arrives last on the tile's counter
+//     adds all partials (any number of pieces).
 struct SplitTile {
   int32_t block, m0, n0, kind;
   int32_t kb, ke, slot, nsplit;
@@ -632,7 +644,7 @@ template <int S, bool CL>
 __global__ void __launch_bounds__(kTcThreads, 1)
     gemm_split_tc_kernel(const GBlock *__restrict__ blocks, const SplitTile *__restrict__ tiles,
                          const int8_t *__restrict__ ws, int cplx, double *__restrict__ C, CDbl alpha,
-                         CDbl beta, int *err, double *__restrict__ part, int *__restrict__ pcnt) {
+                         CDbl beta, int *err, double *__restrict__ part, int *__restrict__ pcnt, int spin) {
   constexpr uint32_t A_BYTES = S * PANEL_A * KSTAGE, B_BYTES = S * PANEL_B * KSTAGE;
   constexpr uint32_t STAGE = A_BYTES + B_BYTES;
   extern __shared__ __align__(1024) unsigned char smem[];
@@ -845,9 +857,11 @@ __global__ void __launch_bounds__(kTcThreads, 1)
         }
       }
     }
-    cluster_arrive();
-    cluster_wait();
+    // a cluster holds either the pieces of one split tile or unsplit tiles only, so `split`
+    // is uniform over the cluster: clusters of unsplit tiles skip both barriers
     if (split) {
+      cluster_arrive();
+      cluster_wait();
       const uint32_t pb = smem_u32(P) + (uint32_t)row * 8u;
 #pragma unroll 1
       for (int c = tile.sid + half * tile.nsplit; c < 4; c += 2 * tile.nsplit) {
@@ -865,21 +879,31 @@ __global__ void __launch_bounds__(kTcThreads, 1)
         }
         final_store(c, v);
       }
+      // no CTA leaves while a peer may still read its partial
+      cluster_arrive();
+      cluster_wait();
     }
-    // no CTA leaves while a peer may still read its partial
-    cluster_arrive();
-    cluster_wait();
   } else {
-  // Pass 0 (split tiles): recombine and store this CTA's FP64 partial tile; the CTA that
-  // arrives last on the tile's counter runs pass 1 with the partials added in split order.
-  // Pass 1: final values to C. One loop body, so each step is emitted once.
+  // Pass 0 (split tiles): recombine and store this CTA's FP64 partial tile. Pass 1 adds the
+  // partials in split order (deterministic) and writes C:
+  //   spin (the launch is one wave, one CTA per SM, so all pieces are resident): every piece
+  //     waits (bounded) until all partials are stored, then takes its share of the column
+  //     chunks (sid, sid + nsplit, …);
+  //   otherwise the piece that arrives last on the tile's counter does all chunks.
+  // Unsplit tiles run pass 1 on their own diagonals. One loop body, so each step is emitted
+  // once.
   double *mine = part + (int64_t)(tile.pbase + tile.sid) * (64 * 128);  // [col][row]
-  int pass = tile.nsplit > 1 ? 0 : 1;
+  const bool split = tile.nsplit > 1;
+  int pass = split ? 0 : 1;
   while (true) {
+    const bool share = pass == 1 && split && spin;
+    const int c0 = share ? tile.sid + half * tile.nsplit : 2 * half;
+    const int cstep = share ? 2 * tile.nsplit : 1;
+    const int cend = share ? 4 : 2 * half + 2;
 #pragma unroll 1
-    for (int c = 2 * half; c < 2 * half + 2; ++c) {
+    for (int c = c0; c < cend; c += cstep) {
       double v[16];
-      if (pass == 0 || tile.nsplit == 1) {
+      if (pass == 0 || !split) {
         recombine(c, v);
       } else {
 #pragma unroll
@@ -901,17 +925,25 @@ __global__ void __launch_bounds__(kTcThreads, 1)
         final_store(c, v);
       }
     }
-    if (pass == 1) {
-      if (tile.nsplit > 1 && tid == 0) pcnt[tile.slot] = 0;
-      break;
-    }
+    if (pass == 1) break;
     __threadfence();
     __syncthreads();
-    if (tid == 0) *ticket = atomicAdd(&pcnt[tile.slot], 1);
+    if (tid == 0) {
+      *ticket = atomicAdd(&pcnt[2 * tile.slot], 1);
+      if (spin && !wait_count(&pcnt[2 * tile.slot], tile.nsplit)) atomicExch(err, 3);
+    }
     __syncthreads();
-    if (*ticket != tile.nsplit - 1) break;
+    if (!spin && *ticket != tile.nsplit - 1) break;
     __threadfence();
     pass = 1;
+  }
+  // counters back to zero for the next launch: by the last piece through pass 1 (spin), or by
+  // the piece that ran it
+  if (split && tid == 0 && pass == 1) {
+    if (!spin || atomicAdd(&pcnt[2 * tile.slot + 1], 1) == tile.nsplit - 1) {
+      pcnt[2 * tile.slot] = 0;
+      pcnt[2 * tile.slot + 1] = 0;
+    }
   }
   }
   tc_fence_before();
@@ -1147,7 +1179,7 @@ int launch_split(tkb_ctx *ctx, const tkb_plan *p, void *C, const void *A, const 
     cfg.numAttrs = na;
     TKB_CUDA_TRY(ctx, cudaLaunchKernelEx(&cfg, k, (const GBlock *)p->blocks, (const SplitTile *)p->kstiles,
                                          (const int8_t *)ctx->ws, cplx, (double *)C, a, b, ctx->counters + 8,
-                                         p->part, p->pcnt));
+                                         p->part, p->pcnt, p->kspin));
   }
   ctx->launches++;
   TKB_CUDA_TRY(ctx, cudaGetLastError());
@@ -1236,10 +1268,10 @@ int max_clusters(int S, int cs, cudaStream_t st) {
 
 // Cluster split plan: tiles with more than T stages are cut into cs pieces (one cluster each),
 // the others are grouped cs per cluster in order of decreasing K (padded with idle CTAs).
-// Cost model (tenths of a K stage of about 1.1 us, from the measured epilogues): a K stage 10,
+// Cost model (tenths of a K stage of about 1 us, from the measured epilogues): a K stage 10,
 // the epilogue of an unsplit tile 30, of a cluster-reduced piece 48, of a global-memory-reduced
-// piece 63 + 6 per piece beyond two.
-constexpr int64_t kCostStage = 10, kCostEpi = 30, kCostEpiCluster = 48, kCostEpiGlobal = 63, kCostEpiGlobalPiece = 6;
+// piece 57 + 3 per piece beyond two.
+constexpr int64_t kCostStage = 10, kCostEpi = 30, kCostEpiCluster = 48, kCostEpiGlobal = 57, kCostEpiGlobalPiece = 3;
 struct ClusterPlan {
   int cs = 0;
   int64_t T = 0, cost = INT64_MAX, ctas = 0;
@@ -1476,6 +1508,8 @@ int tkb_gemm_split_prepare(tkb_ctx *ctx, tkb_plan *p) {
   p->ws_bytes = off;
   p->nstiles = (int64_t)tiles.size();
   p->nkstiles = (int64_t)kt.size();
+  // pieces may wait for each other only when every CTA of the launch is resident at once
+  p->kspin = (int64_t)kt.size() <= (int64_t)ctx->num_sms ? 1 : 0;
   p->nsjobs = (int)jobs.size();
   p->nsrows = (int64_t)jobs.size();
   cudaError_t e = cudaSuccess;
@@ -1490,8 +1524,9 @@ int tkb_gemm_split_prepare(tkb_ctx *ctx, tkb_plan *p) {
   if (e == cudaSuccess && nslots > 0) {
     const size_t pb = (size_t)npart * 64 * 128 * sizeof(double);
     e = cudaMalloc((void **)&p->part, pb);
-    if (e == cudaSuccess) e = cudaMalloc((void **)&p->pcnt, nslots * sizeof(int));
-    if (e == cudaSuccess) e = cudaMemset(p->pcnt, 0, nslots * sizeof(int));
+    // per slot: arrival counter and completion counter (reset by the last piece)
+    if (e == cudaSuccess) e = cudaMalloc((void **)&p->pcnt, 2 * nslots * sizeof(int));
+    if (e == cudaSuccess) e = cudaMemset(p->pcnt, 0, 2 * nslots * sizeof(int));
   }
   if (e == cudaSuccess && !jobs.empty()) {
     e = cudaMalloc(&p->sjobs, jobs.size() * sizeof(SliceTask));

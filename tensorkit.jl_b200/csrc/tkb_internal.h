@@ -193,6 +193,7 @@ struct tkb_plan {
   int *pcnt = nullptr;          // split-K arrival counters (self-clearing)
   int kcluster = 0;             // > 1: split tiles reduced inside clusters of this many CTAs
   int slice_lk = 16;            // K values per lane in the slicing pass's warp tiles (8 or 16)
+  int kspin = 0;                // split-K pieces wait for each other (the launch is one wave)
   void *sjobs = nullptr;        // slice jobs (block, operand)
   int64_t *srow_begin = nullptr;
   int nsjobs = 0;

@@ -98,3 +98,19 @@ def test_split_k_reductions(cplx, monkeypatch):
         tk.mul_(Cd, Ad, Bd, 0.5, -2.0, prec="split")
         assert relerr(Cd.to_host(), want) <= TOL_SPLIT
     ctx.empty_caches()
+
+
+def test_split_long_k_multiwave():
+    """K beyond the exact int32 range of one product task (≈ 19K positions at 7 slices) forces
+    at least two pieces per tile; with more pieces than SMs the launch is not one wave, so the
+    pieces do not wait for each other and the last one to arrive adds the partials."""
+    Vm = O.Space({O.U1(0): 1024})
+    Vk = O.Space({O.U1(0): 20000})
+    Vn = O.Space({O.U1(0): 640})
+    A = O.randn(O.Hom([Vm], [Vk]), 11)
+    B = O.randn(O.Hom([Vk], [Vn]), 12)
+    ref = O.mul(A, B)
+    Ad, Bd = to_device(A), to_device(B)
+    C = tk.TensorMap.zeros(to_hom(ref.W), dtype=Ad.dtype, device=Ad.device)
+    tk.mul_(C, Ad, Bd, 1.0, 0.0, prec="split")
+    assert relerr(C.to_host(), ref.data) <= TOL_SPLIT
