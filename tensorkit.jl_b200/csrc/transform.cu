@@ -21,6 +21,9 @@
 #include <cstring>
 #include <numeric>
 
+#include <mutex>
+#include <unordered_map>
+
 #include "tkb_internal.h"
 
 namespace {
@@ -341,6 +344,23 @@ __global__ void __launch_bounds__(kThreads)
 bool use_plain_transform() {
   const char *e = std::getenv("TKB_TRANSFORM_KERNEL");
   return e && std::strcmp(e, "plain") == 0;
+}
+
+// CTAs per SM of a pipelined transform kernel: the shared-memory attribute is set and the
+// occupancy queried once per kernel (the shared memory size is fixed per element type), so
+// eager launches make no attribute calls (per device: attributes belong to the device's context)
+int pipe_occupancy(int device, const void *kfn, size_t smem) {
+  static std::mutex mu;
+  static std::unordered_map<const void *, int> cache[64];
+  if (device < 0 || device >= 64) return 0;
+  std::lock_guard<std::mutex> lock(mu);
+  auto it = cache[device].find(kfn);
+  if (it != cache[device].end()) return it->second;
+  if (cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) return 0;
+  int per_sm = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kfn, kThreads, smem) != cudaSuccess) return 0;
+  cache[device][kfn] = per_sm;
+  return per_sm;
 }
 
 int64_t pow2ceil(int64_t x) {
@@ -695,9 +715,8 @@ int tkb_transform_launch(tkb_ctx *ctx, const tkb_table *t, int dtype, void *dst,
                             : treetransform_pipe_kernel<double2, false, int64_t>);
       kfn = (const void *)kc;
     }
-    TKB_CUDA_TRY(ctx, cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    int per_sm = 1;
-    TKB_CUDA_TRY(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kfn, kThreads, smem));
+    const int per_sm = pipe_occupancy(ctx->device, kfn, smem);
+    if (per_sm <= 0) return tkb_set_error(ctx, TKB_ERR_CUDA, "pipelined transform: occupancy query failed");
     int64_t pg = std::min<int64_t>(t->ntasks, (int64_t)ctx->num_sms * std::max(1, per_sm));
     pg = std::max<int64_t>(pg, (t->ntasks + kRecCache - 1) / kRecCache);
     const int pgrid = (int)pg;
