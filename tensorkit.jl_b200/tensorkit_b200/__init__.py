@@ -23,5 +23,7 @@ from .tensoroperations import (tensoradd_, tensorcontract_, tensorcontract, cont
                                tensortrace_, tensortrace, tensortrace_structure)
 from .trace import trace_permute_, trace_permute
 from .network import NetworkPlan
+from . import storage
+from .storage import to_dict, from_dict
 
 __version__ = "0.1.0"
