@@ -25,5 +25,9 @@ from .trace import trace_permute_, trace_permute
 from .network import NetworkPlan
 from . import storage
 from .storage import to_dict, from_dict
+from . import factorizations
+from .factorizations import (svd_compact, svd_vals, svd_trunc, qr_compact, lq_compact, eigh_full,
+                             eigh_vals, eigh_trunc, notrunc, truncrank, trunctol, truncerror,
+                             truncspace)
 
 __version__ = "0.1.0"
