@@ -469,6 +469,8 @@ def main():
     ap.add_argument("--workload", default="su2_large", choices=sorted(WORKLOADS))
     ap.add_argument("--kernel-only", default=None, choices=["transform", "gemm"],
                     help="profiling aid: one eager step, then relaunch the largest kernel of this kind")
+    ap.add_argument("--factor", default=None, choices=["svd_trunc", "qr_compact", "eigh_full"],
+                    help="time one block factorization of the workload's first input instead")
     ap.add_argument("--precision", default="split", choices=["split", "plain"])
     ap.add_argument("--reps", type=int, default=3)
     args = ap.parse_args()
@@ -478,6 +480,8 @@ def main():
         return run_reference(args)
     if args.kernel_only:
         return run_kernel_only(args)
+    if args.factor:
+        return run_factor(args)
     return run_ours(args)
 
 
@@ -512,6 +516,49 @@ def run_kernel_only(args):
     ctx.stream.synchronize()
     print(json.dumps({"kernel_only": kind, "workload": args.workload, "preceding_launches": len(cands),
                       "reps": args.reps, **size}))
+    return 0
+
+
+def run_factor(args):
+    """One block factorization of the workload's first input tensor (eigh: of t†t), device time
+    with CUDA events over --steps calls, beside numpy/LAPACK on the same blocks on the host."""
+    import numpy as np
+    import torch
+    import tensorkit_b200 as tk
+    from helpers import from_sector, to_device
+    from oracle import factor as F
+
+    dev = torch.device("cuda", 0)
+    ot = next(iter(oracle_inputs(args.workload).values()))
+    t = to_device(ot, dev)
+    if args.factor == "eigh_full":
+        t = tk.compose(t.adjoint(), t)
+        oblocks = {from_sector(c): t.block(c).cpu().numpy() for c in t.blocksectors()}
+    else:
+        oblocks = {from_sector(c): ot.block(from_sector(c)) for c in t.blocksectors()}
+    fn = {"svd_trunc": lambda: tk.svd_trunc(t, tk.truncrank(t.space.domain.dim() // 2)),
+          "qr_compact": lambda: tk.qr_compact(t), "eigh_full": lambda: tk.eigh_full(t)}[args.factor]
+    npfn = {"svd_trunc": lambda b: np.linalg.svd(b, full_matrices=False),
+            "qr_compact": lambda b: np.linalg.qr(b), "eigh_full": lambda b: np.linalg.eigh(b)}[args.factor]
+    for _ in range(args.warmup):
+        fn()
+    torch.cuda.synchronize()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record()
+    for _ in range(args.steps):
+        fn()
+    b.record()
+    torch.cuda.synchronize()
+    ms = a.elapsed_time(b) / args.steps
+    t0 = time.perf_counter()
+    for blk in oblocks.values():
+        npfn(blk)
+    cpu_ms = (time.perf_counter() - t0) * 1e3
+    shapes = sorted({tuple(v.shape) for v in oblocks.values()})
+    print(json.dumps({"factor": args.factor, "workload": args.workload, "blocks": len(oblocks),
+                      "block_shapes": shapes[-3:], "ms_per_call": ms, "cpu_numpy_ms": cpu_ms,
+                      "steps": args.steps, "note": "per-block vendor solver (torch.linalg / cuSOLVER), "
+                                                   "batched over equal block shapes"}))
     return 0
 
 

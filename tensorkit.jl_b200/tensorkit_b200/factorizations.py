@@ -96,10 +96,14 @@ def _diag(V: GradedSpace, vals: SectorVector, like, dtype):
 
 
 # ---- SVD -----------------------------------------------------------------------------------
+SVD_DRIVER = None  # cuSOLVER driver for device SVDs (None: torch's default; "gesvdj": Jacobi)
+
+
 def _svd_blocks(t):
     import torch
     blocks = {c: t.block(c) for c in t.blocksectors()}
-    return _batched(blocks, lambda x: torch.linalg.svd(x, full_matrices=False))
+    drv = SVD_DRIVER if t.data.is_cuda else None
+    return _batched(blocks, lambda x: torch.linalg.svd(x, full_matrices=False, driver=drv))
 
 
 def svd_compact(t):
