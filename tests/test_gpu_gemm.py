@@ -114,3 +114,20 @@ def test_split_long_k_multiwave():
     C = tk.TensorMap.zeros(to_hom(ref.W), dtype=Ad.dtype, device=Ad.device)
     tk.mul_(C, Ad, Bd, 1.0, 0.0, prec="split")
     assert relerr(C.to_host(), ref.data) <= TOL_SPLIT
+
+
+@pytest.mark.parametrize("cplx", [False, True])
+def test_split_many_short_k_tasks(cplx):
+    """Hundreds of 32-row slicing tasks with short K (more clusters than fit at once, so the
+    slicing pass runs in several waves); op(A) rows and op(B) columns through both load layouts
+    (B given as Bᴴ)."""
+    Vm = O.Space({O.U1(0): 24000, O.U1(1): 300})
+    Vk = O.Space({O.U1(0): 128, O.U1(1): 40})
+    Vn = O.Space({O.U1(0): 96, O.U1(1): 20})
+    A = O.randn(O.Hom([Vm], [Vk]), 21, cplx)
+    Bt = O.randn(O.Hom([Vn], [Vk]), 22, cplx)
+    ref = O.mul(A, Bt, adjB=True)
+    Ad, Btd = to_device(A), to_device(Bt)
+    C = tk.TensorMap.zeros(to_hom(ref.W), dtype=Ad.dtype, device=Ad.device)
+    tk.mul_(C, Ad, tk.AdjointTensorMap(Btd), 1.0, 0.0, prec="split")
+    assert relerr(C.to_host(), ref.data) <= TOL_SPLIT
