@@ -202,6 +202,47 @@ __device__ __forceinline__ bool load_tile(int t, const typename SrcVal<CPLX>::T 
   }
 }
 
+// Phase-1 row maxima of warp tile t of a K-contiguous source (the layout load_tile stages):
+// each lane reduces its own values per row, then the warp takes the maximum per row with two
+// 32-bit max-reductions (high word, then low word among the lanes holding the high maximum;
+// the bits of non-negative doubles order like their values). No staging, so the loads of
+// consecutive tiles can overlap.
+template <bool CPLX, int LK>
+__device__ __forceinline__ void tile_rowmax_kc(int t, const typename SrcVal<CPLX>::T *__restrict__ X, int64_t xo,
+                                               int64_t rs, int64_t r0, int64_t msrc, int64_t ksrc, int lane,
+                                               unsigned long long *rmax) {
+  using T = typename SrcVal<CPLX>::T;
+  const T z = zero_of(T{});
+  constexpr int RG = CPLX ? 8 : 4;
+  constexpr int KW = (CPLX ? 4 : 8) * LK;
+  constexpr int NH = KW / 32;
+  const int ngrp = 32 / RG;
+  const int grp = t % ngrp;
+  const int64_t k0 = (int64_t)(t / ngrp) * KW;
+  double m[RG];
+#pragma unroll
+  for (int rr = 0; rr < RG; ++rr) {
+    const int64_t r = r0 + grp * RG + rr;
+    const bool rv = r < msrc;
+    const T *p = X + xo + r * rs;
+    double mm = 0.0;
+#pragma unroll
+    for (int h = 0; h < NH; ++h) {
+      const int64_t l = k0 + 32 * h + lane;
+      mm = fmax(mm, absmax((rv && l < ksrc) ? __ldg(p + l) : z));
+    }
+    m[rr] = mm;
+  }
+#pragma unroll
+  for (int rr = 0; rr < RG; ++rr) {
+    const unsigned hi = (unsigned)__double2hiint(m[rr]), lo = (unsigned)__double2loint(m[rr]);
+    const unsigned H = __reduce_max_sync(0xffffffffu, hi);
+    const unsigned L = __reduce_max_sync(0xffffffffu, hi == H ? lo : 0u);
+    if (lane == rr && (H | L) != 0u)
+      atomicMax(&rmax[grp * RG + rr], ((unsigned long long)H << 32) | (unsigned long long)L);
+  }
+}
+
 // Integer slicing. The row exponent e is the binary exponent of the row maximum m
 // (m = f·2^e, f in [0.5, 1)), raised by one when round(f·2^(7S)) would reach 2^(7S), so that
 // Y = round(|v|·2^(7S−e)) < 2^(7S) for every v of the row. Y is read from the mantissa of
@@ -328,12 +369,17 @@ __device__ __forceinline__ void slice_task(const GBlock &b, const SliceTask &tas
 
   // phase 1: row maxima of this CTA's tiles. With 8-K real tiles the warp's first tile stays
   // in registers for phase 2 (most warps have one tile).
-  constexpr bool KEEP = LK == 8 && !CPLX;
+  constexpr bool KEEP = LK == 8 && !CPLX && ROWC;
   T keep[KEEP ? LK : 1];
   int krow = 0;
   int64_t kc = 0;
   bool kok = false;
+#pragma unroll 2
   for (int t = t0; t < ntile; t += tstep) {
+    if constexpr (!ROWC) {
+      tile_rowmax_kc<CPLX, LK>(t, X, xo, rs, r0, msrc, b.k, lane, rmax);
+      continue;
+    }
     T v[LK];
     int row;
     int64_t c;
