@@ -145,34 +145,34 @@ __device__ __forceinline__ double2 zero_of(double2) { return make_double2(0.0, 0
 __device__ __forceinline__ double absmax(double v) { return fabs(v); }
 __device__ __forceinline__ double absmax(double2 v) { return fmax(fabs(v.x), fabs(v.y)); }
 
-// Loads warp tile t into v[LK]; returns the lane's source row (relative to the task) and the
-// source K of v[0] through row/c; false when the lane's piece lies beyond the padded K.
+// Warp tile t in two steps: fetch_tile issues the global loads into f[LK] (rows contiguous:
+// the lane's row, K-contiguous: RG rows × NH values along K per lane, lanes along K), and
+// unpack_tile turns them into v[LK] = LK consecutive K values of one source row, staging the
+// K-contiguous layout through the warp's shared-memory tile. unpack returns the lane's source
+// row (relative to the task) and the source K of v[0] through row/c, and false when the lane's
+// piece lies beyond the padded K. Splitting the two lets a warp fetch its next tile while it
+// slices the current one.
 template <bool CPLX, bool ROWC, int LK>
-__device__ __forceinline__ bool load_tile(int t, const typename SrcVal<CPLX>::T *__restrict__ X,
-                                          int64_t xo, int64_t rs, int64_t ks, int64_t r0,
-                                          int64_t msrc, int64_t ksrc, int64_t kfull,
-                                          typename SrcVal<CPLX>::T *stage, int lane,
-                                          typename SrcVal<CPLX>::T (&v)[LK], int &row, int64_t &c) {
+__device__ __forceinline__ void fetch_tile(int t, const typename SrcVal<CPLX>::T *__restrict__ X, int64_t xo,
+                                           int64_t rs, int64_t ks, int64_t r0, int64_t msrc, int64_t ksrc,
+                                           int lane, typename SrcVal<CPLX>::T (&f)[LK]) {
   using T = typename SrcVal<CPLX>::T;
   const T z = zero_of(T{});
   if constexpr (ROWC) {
-    row = lane;
-    c = LK * (int64_t)t;
+    const int64_t c = LK * (int64_t)t;
     const int64_t r = r0 + lane;
     const bool rv = r < msrc;
     const T *p = X + xo + r * rs;
 #pragma unroll
-    for (int q = 0; q < LK; ++q) v[q] = (rv && c + q < ksrc) ? __ldg(p + (c + q) * ks) : z;
-    return true;
+    for (int q = 0; q < LK; ++q) f[q] = (rv && c + q < ksrc) ? __ldg(p + (c + q) * ks) : z;
   } else {
-    constexpr int RG = CPLX ? 8 : 4;       // rows per warp tile
+    constexpr int RG = CPLX ? 8 : 4;         // rows per warp tile
     constexpr int KW = (CPLX ? 4 : 8) * LK;  // K per warp tile
-    constexpr int NH = KW / 32;            // loads per row per lane
-    constexpr int RP = (KW / LK) * (LK + 1);  // staging row pitch (elements)
+    constexpr int NH = KW / 32;              // loads per row per lane
+    static_assert(RG * NH == LK, "one fetched value per unpacked value");
     const int ngrp = 32 / RG;
     const int grp = t % ngrp;
     const int64_t k0 = (int64_t)(t / ngrp) * KW;
-    T tmp[RG * NH];
 #pragma unroll
     for (int rr = 0; rr < RG; ++rr) {
       const int64_t r = r0 + grp * RG + rr;
@@ -181,15 +181,35 @@ __device__ __forceinline__ bool load_tile(int t, const typename SrcVal<CPLX>::T 
 #pragma unroll
       for (int h = 0; h < NH; ++h) {
         const int64_t l = k0 + 32 * h + lane;
-        tmp[rr * NH + h] = (rv && l < ksrc) ? __ldg(p + l) : z;
+        f[rr * NH + h] = (rv && l < ksrc) ? __ldg(p + l) : z;
       }
     }
+  }
+}
+template <bool CPLX, bool ROWC, int LK>
+__device__ __forceinline__ bool unpack_tile(int t, const typename SrcVal<CPLX>::T (&f)[LK], int64_t kfull,
+                                            typename SrcVal<CPLX>::T *stage, int lane,
+                                            typename SrcVal<CPLX>::T (&v)[LK], int &row, int64_t &c) {
+  if constexpr (ROWC) {
+#pragma unroll
+    for (int q = 0; q < LK; ++q) v[q] = f[q];
+    row = lane;
+    c = LK * (int64_t)t;
+    return true;
+  } else {
+    constexpr int RG = CPLX ? 8 : 4;
+    constexpr int KW = (CPLX ? 4 : 8) * LK;
+    constexpr int NH = KW / 32;
+    constexpr int RP = (KW / LK) * (LK + 1);  // staging row pitch (elements)
+    const int ngrp = 32 / RG;
+    const int grp = t % ngrp;
+    const int64_t k0 = (int64_t)(t / ngrp) * KW;
     __syncwarp();
 #pragma unroll
     for (int rr = 0; rr < RG; ++rr)
 #pragma unroll
       for (int h = 0; h < NH; ++h)
-        stage[rr * RP + ((32 / LK) * h + lane / LK) * (LK + 1) + lane % LK] = tmp[rr * NH + h];
+        stage[rr * RP + ((32 / LK) * h + lane / LK) * (LK + 1) + lane % LK] = f[rr * NH + h];
     __syncwarp();
     constexpr int LPR = 32 / RG;  // lanes per row
     static_assert(LPR * LK == KW, "one warp tile row is read back by LPR lanes");
@@ -200,6 +220,16 @@ __device__ __forceinline__ bool load_tile(int t, const typename SrcVal<CPLX>::T 
     c = k0 + LK * kap;
     return c < kfull;
   }
+}
+template <bool CPLX, bool ROWC, int LK>
+__device__ __forceinline__ bool load_tile(int t, const typename SrcVal<CPLX>::T *__restrict__ X,
+                                          int64_t xo, int64_t rs, int64_t ks, int64_t r0,
+                                          int64_t msrc, int64_t ksrc, int64_t kfull,
+                                          typename SrcVal<CPLX>::T *stage, int lane,
+                                          typename SrcVal<CPLX>::T (&v)[LK], int &row, int64_t &c) {
+  typename SrcVal<CPLX>::T f[LK];
+  fetch_tile<CPLX, ROWC, LK>(t, X, xo, rs, ks, r0, msrc, ksrc, lane, f);
+  return unpack_tile<CPLX, ROWC, LK>(t, f, kfull, stage, lane, v, row, c);
 }
 
 // Phase-1 row maxima of warp tile t of a K-contiguous source (the layout load_tile stages):
@@ -371,9 +401,6 @@ __device__ __forceinline__ void slice_task(const GBlock &b, const SliceTask &tas
   // in registers for phase 2 (most warps have one tile).
   constexpr bool KEEP = LK == 8 && !CPLX && ROWC;
   T keep[KEEP ? LK : 1];
-  int krow = 0;
-  int64_t kc = 0;
-  bool kok = false;
 #pragma unroll 2
   for (int t = t0; t < ntile; t += tstep) {
     if constexpr (!ROWC) {
@@ -388,9 +415,6 @@ __device__ __forceinline__ void slice_task(const GBlock &b, const SliceTask &tas
       if (t == t0) {
 #pragma unroll
         for (int q = 0; q < LK; ++q) keep[q] = v[q];
-        krow = row;
-        kc = c;
-        kok = ok;
       }
     }
     double m = 0.0;
@@ -429,20 +453,25 @@ __device__ __forceinline__ void slice_task(const GBlock &b, const SliceTask &tas
   const int64_t kpad = b.kpad;
   int8_t *base = ws + (op == 0 ? b.wsA : b.wsB);
   const int64_t plane = (int64_t)pr * KSTAGE;  // between the slices of one stage
+  // the next tile is fetched before the current one is sliced (its loads overlap the work)
+  T nxt[LK];
+  if (t0 < ntile) {
+    if (KEEP) {
+#pragma unroll
+      for (int q = 0; q < LK; ++q) nxt[q] = keep[KEEP ? q : 0];
+    } else {
+      fetch_tile<CPLX, ROWC, LK>(t0, X, xo, rs, ks, r0, msrc, b.k, lane, nxt);
+    }
+  }
   for (int t = t0; t < ntile; t += tstep) {
+    T cur[LK];
+#pragma unroll
+    for (int q = 0; q < LK; ++q) cur[q] = nxt[q];
+    if (t + tstep < ntile) fetch_tile<CPLX, ROWC, LK>(t + tstep, X, xo, rs, ks, r0, msrc, b.k, lane, nxt);
     T v[LK];
     int row;
     int64_t c;
-    bool ok;
-    if (KEEP && t == t0) {
-#pragma unroll
-      for (int q = 0; q < LK; ++q) v[q] = keep[KEEP ? q : 0];
-      row = krow;
-      c = kc;
-      ok = kok;
-    } else {
-      ok = load_tile<CPLX, ROWC, LK>(t, X, xo, rs, ks, r0, msrc, b.k, kfull, stage, lane, v, row, c);
-    }
+    const bool ok = unpack_tile<CPLX, ROWC, LK>(t, cur, kfull, stage, lane, v, row, c);
     if (!ok) continue;
     const RowScale rsc = row_scale<S>(rexp[row]);
     const int64_t r = r0 + row;
