@@ -680,8 +680,15 @@ __device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::
 
 constexpr uint32_t kTmemCols = 512;
 // instruction descriptor: D s32 (bits 4-5 = 2), A/B signed int8 (bits 7-9, 10-12 = 1),
-// both K-major, N = 64 (bits 17-22 = 64>>3), M = 128 (bits 24-28 = 128>>4)
-constexpr uint32_t kIdescI8 = (2u << 4) | (1u << 7) | (1u << 10) | ((64u >> 3) << 17) | ((128u >> 4) << 24);
+// both K-major, N (bits 17-22 = N>>3), M = 128 (bits 24-28 = 128>>4)
+__host__ __device__ constexpr uint32_t idesc_i8(uint32_t n) {
+  return (2u << 4) | (1u << 7) | (1u << 10) | ((n >> 3) << 17) | ((128u >> 4) << 24);
+}
+// B slices per product: the products (s, t), (s, t+1), … share the A slice s and land in the
+// adjacent diagonals s+t, s+t+1, … of TMEM; the B slices of a stage lie back to back (2 KiB,
+// i.e. 64 rows, each, with the same 256-byte step between 8-row groups), so up to four of them
+// form one N ≤ 256 operand and one instruction computes the four products.
+constexpr int kMaxSlicesPerMma = 4;
 
 // One product task: output tile (m0, n0) of a block, K stages [kb, ke). When a tile's K
 // range is split over nsplit CTAs (few tiles, long K), each CTA recombines its own int32
@@ -804,8 +811,11 @@ __global__ void __launch_bounds__(kTcThreads, 1)
 #pragma unroll
       for (int s = 0; s < S; ++s) {
 #pragma unroll
-        for (int t = 0; t < S - s; ++t)
-          umma_i8(tmem + (uint32_t)((s + t) * 64), ad[s], bd[t], kIdescI8, (kt > 0 || s > 0) ? 1u : 0u);
+        for (int t = 0; t < S - s; t += kMaxSlicesPerMma) {
+          const int nsl = (S - s - t) < kMaxSlicesPerMma ? (S - s - t) : kMaxSlicesPerMma;
+          umma_i8(tmem + (uint32_t)((s + t) * 64), ad[s], bd[t], idesc_i8(64u * (uint32_t)nsl),
+                  (kt > 0 || s > 0) ? 1u : 0u);
+        }
       }
       umma_commit(&empty[st]);
       if (kt >= 1) {
