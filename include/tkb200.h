@@ -64,7 +64,15 @@ int tkb_version(void);
 int tkb_ctx_create(int device, void *stream, size_t workspace_bytes, tkb_ctx **out);
 int tkb_ctx_destroy(tkb_ctx *ctx);
 int tkb_ctx_set_stream(tkb_ctx *ctx, void *stream);
+/* Waits for the context's stream. Returns TKB_ERR_TIMEOUT (and clears the record) when a
+ * bounded device wait of an earlier launch on this context gave up; tkb_last_error names it. */
 int tkb_ctx_synchronize(tkb_ctx *ctx);
+/* Diagnostic (no counterpart in the reference): launches one kernel that waits on a device
+ * flag that nothing sets, for at most timeout_us microseconds (1 .. 1000000), and records the
+ * timeout like any bounded device wait of the library; the next tkb_ctx_synchronize reports
+ * TKB_ERR_TIMEOUT and the context stays usable. It exercises the error path of the bounded
+ * waits without faulting the GPU. */
+int tkb_selftest_bounded_wait(tkb_ctx *ctx, int64_t timeout_us);
 /* kernels launched by this context since creation (for launch accounting) */
 int tkb_ctx_launch_count(const tkb_ctx *ctx, int64_t *count);
 const char *tkb_last_error(const tkb_ctx *ctx);

@@ -97,9 +97,57 @@ int tkb_ctx_set_stream(tkb_ctx *ctx, void *stream) {
   return TKB_OK;
 }
 
+// ctx->counters[kErrSlot]: codes of bounded device waits that gave up (kernels set it with
+// atomicExch, the host reads and clears it at synchronisation)
+constexpr int kErrSlot = 8, kNeverSetSlot = 10;
+
 int tkb_ctx_synchronize(tkb_ctx *ctx) {
   if (!ctx) return tkb_set_error(nullptr, TKB_ERR_ARG, "null context");
   TKB_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+  int code = 0;
+  TKB_CUDA_TRY(ctx, cudaMemcpyAsync(&code, ctx->counters + kErrSlot, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+  TKB_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+  if (code != 0) {
+    TKB_CUDA_TRY(ctx, cudaMemsetAsync(ctx->counters + kErrSlot, 0, sizeof(int), ctx->stream));
+    TKB_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+    static const char *what[] = {"", "split GEMM: a shared-memory ring stage did not arrive",
+                                 "split GEMM: the tensor-core products did not complete",
+                                 "split GEMM: the split-K pieces of a tile did not all arrive",
+                                 "bounded-wait self-test: the flag was never set"};
+    return tkb_set_error(ctx, TKB_ERR_TIMEOUT,
+                         std::string("bounded device wait gave up: ") + (code >= 1 && code <= 4 ? what[code] : "unknown"));
+  }
+  return TKB_OK;
+}
+
+namespace {
+// one thread waits (bounded by %globaltimer) on a flag that nothing sets, then records code 4
+__global__ void bounded_wait_selftest_kernel(const int *flag, int *err, long long timeout_ns) {
+  if (threadIdx.x != 0) return;
+  unsigned long long t0;
+  asm volatile("mov.u64 %0, %%globaltimer;\n" : "=l"(t0));
+  while (true) {
+    int v;
+    asm volatile("ld.acquire.gpu.global.s32 %0, [%1];\n" : "=r"(v) : "l"(flag) : "memory");
+    if (v != 0) return;
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;\n" : "=l"(t));
+    if ((long long)(t - t0) > timeout_ns) {
+      atomicExch(err, 4);
+      return;
+    }
+    __nanosleep(1000);
+  }
+}
+}  // namespace
+
+int tkb_selftest_bounded_wait(tkb_ctx *ctx, int64_t timeout_us) {
+  if (!ctx) return tkb_set_error(nullptr, TKB_ERR_ARG, "null context");
+  if (timeout_us < 1 || timeout_us > 1000000) return tkb_set_error(ctx, TKB_ERR_ARG, "timeout_us must be in 1 .. 1000000");
+  bounded_wait_selftest_kernel<<<1, 32, 0, ctx->stream>>>(ctx->counters + kNeverSetSlot, ctx->counters + kErrSlot,
+                                                          (long long)timeout_us * 1000);
+  ctx->launches++;
+  TKB_CUDA_TRY(ctx, cudaGetLastError());
   return TKB_OK;
 }
 

@@ -24,7 +24,8 @@ TKB_NORM2, TKB_INNER, TKB_TRACE = 0, 1, 2
 
 EXPORTS = [
     "tkb_version", "tkb_ctx_create", "tkb_ctx_destroy", "tkb_ctx_set_stream",
-    "tkb_ctx_synchronize", "tkb_ctx_launch_count", "tkb_last_error", "tkb_table_create",
+    "tkb_ctx_synchronize", "tkb_selftest_bounded_wait", "tkb_ctx_launch_count", "tkb_last_error",
+    "tkb_table_create",
     "tkb_table_destroy", "tkb_table_info", "tkb_treetransform", "tkb_trace_table_create",
     "tkb_trace_table_destroy", "tkb_tracetransform", "tkb_gemm_plan_create",
     "tkb_gemm_plan_destroy", "tkb_gemm_plan_info", "tkb_grouped_gemm", "tkb_rplan_create",
@@ -88,6 +89,7 @@ def _declare(lib):
         "tkb_ctx_destroy": ([vp], C.c_int),
         "tkb_ctx_set_stream": ([vp, vp], C.c_int),
         "tkb_ctx_synchronize": ([vp], C.c_int),
+        "tkb_selftest_bounded_wait": ([vp, i64], C.c_int),
         "tkb_ctx_launch_count": ([vp, P(i64)], C.c_int),
         "tkb_last_error": ([vp], C.c_char_p),
         "tkb_table_create": ([vp, P(tkb_table_desc), P(vp)], C.c_int),
