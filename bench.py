@@ -196,6 +196,23 @@ def workload_flops(name):
 
 
 # ---- our arm -------------------------------------------------------------------------------
+def max_over_ranks(ms, device, world):
+    """The slowest rank's time: every rank takes part in one MAX all-reduce (NCCL on GPUs,
+    gloo on host tensors), so all ranks return the same value."""
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(ms)], dtype=torch.float64, device=device)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def whole_job_value(flops_per_step, world, steps, ms):
+    """GFLOP/s of the whole job: every rank runs `steps` steps of `flops_per_step` (weak scaling,
+    replicas), timed by the slowest rank's `ms` for all its steps."""
+    return flops_per_step * world * steps / (ms * 1e-3) / 1e9
+
+
 def run_ours(args):
     import numpy as np
     import torch
@@ -262,10 +279,7 @@ def run_ours(args):
                 evs.append((a, b))
             stream.synchronize()
             ms = sum(a.elapsed_time(b) for a, b in evs)
-        t = torch.tensor([ms], dtype=torch.float64, device=dev)
-        if world > 1:
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return max_over_ranks(ms, dev, world)
 
     with ClockSampler(local) as clk:
         ms_split = timed(plans["split"], args.steps, args.warmup, clk)
@@ -337,17 +351,14 @@ def run_ours(args):
     e2e_run(args.steps, a, b)
     torch.cuda.synchronize(dev)
     ms_e2e = a.elapsed_time(b)
-    te = torch.tensor([ms_e2e], dtype=torch.float64, device=dev)
-    if world > 1:
-        dist.all_reduce(te, op=dist.ReduceOp.MAX)
-    ms_e2e = float(te.item())
+    ms_e2e = max_over_ranks(ms_e2e, dev, world)
 
     # per-kernel breakdown of one split step; the dominant kernel gives the roofline entry
     roof, breakdown = kernel_roofline(args, logs["split"], ctx, flush) if rank == 0 else (None, None)
 
-    value = flops * world * args.steps / (ms_split * 1e-3) / 1e9
-    plain_value = flops * world * args.steps / (ms_plain * 1e-3) / 1e9
-    e2e_value = flops * world * args.steps / (ms_e2e * 1e-3) / 1e9
+    value = whole_job_value(flops, world, args.steps, ms_split)
+    plain_value = whole_job_value(flops, world, args.steps, ms_plain)
+    e2e_value = whole_job_value(flops, world, args.steps, ms_e2e)
     line = None
     if rank == 0:
         cpu = cpu_baseline(args, tens_o, flops) if world == 1 else None
