@@ -26,14 +26,14 @@
 // copy moves into shared memory (the issue rate of one producer thread, not the copy size,
 // limits the ring).
 //
-// Launches: slicing pass (one thread-block cluster per 32 source rows: row maxima,
-// exponents, slices) + product pass:
+// Launches: slicing pass (32 source rows per task, run by 1–4 CTAs of a thread-block cluster:
+// row maxima, exponents, slices) + product pass:
 //   tcgen05 kernel (default): one CTA per 128×64 output tile (and K range, when the K loop
-//   is split across CTAs); one thread streams the S slice stages of A and B with
-//   cp.async.bulk into a shared-memory ring as deep as fits (5 stages at S = 7) and issues
-//   tcgen05.mma.kind::i8 (M=128, N=64, K=32) into S int32 accumulators held in tensor memory (S·64 of 512
-//   columns); eight warps (two per TMEM lane quarter) read the accumulators back with tcgen05.ld and recombine them in
-//   FP64.
+//   is split across CTAs); one thread streams the stages of A and B with cp.async.bulk into a
+//   shared-memory ring as deep as fits (5 stages at S = 7) and issues tcgen05.mma.kind::i8
+//   (M=128, K=32, N = 64 per B slice, up to four B slices per instruction) into S int32
+//   diagonal accumulators held in tensor memory (S·64 of 512 columns); eight warps (two per
+//   TMEM lane quarter) read the accumulators back with tcgen05.ld and recombine them in FP64.
 //   mma.sync kernel (TKB_SPLIT_KERNEL=mma): the same products with int8 mma.sync.
 #include <algorithm>
 #include <cmath>
@@ -1353,7 +1353,8 @@ int max_clusters(int S, int cs, cudaStream_t st) {
 
 // Cluster split plan: tiles with more than T stages are cut into cs pieces (one cluster each),
 // the others are grouped cs per cluster in order of decreasing K (padded with idle CTAs).
-// Cost model (tenths of a K stage of about 1 us, from the measured epilogues): a K stage 10,
+// Cost model (tenths of a microsecond, from the measured epilogues): a K stage 10 (measured
+// 0.7–1.1 us depending on the MMA grouping; the choices below did not change between the two),
 // the epilogue of an unsplit tile 30, of a cluster-reduced piece 48, of a global-memory-reduced
 // piece 57 + 3 per piece beyond two.
 constexpr int64_t kCostStage = 10, kCostEpi = 30, kCostEpiCluster = 48, kCostEpiGlobal = 57, kCostEpiGlobalPiece = 3;
