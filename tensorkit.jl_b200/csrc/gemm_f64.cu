@@ -378,27 +378,25 @@ __device__ __forceinline__ double2 scl(double2 v, CDbl a) {
 // D bounds n and k of every block of the launch (4, 8 or 16): the row loops are unrolled to D,
 // so the code stays small for the common narrow bonds.
 template <typename T, bool BZ, int D>
-__global__ void __launch_bounds__(kSkinnyRows)
+__global__ void __launch_bounds__(kSkinnyRows, (sizeof(T) == 8 && D <= 8 && BZ) ? 4 : 1)
     gemm_skinny_kernel(const GBlock *__restrict__ blocks, const GTile *__restrict__ tasks, int64_t ntasks,
                        T *__restrict__ C, const T *__restrict__ A, const T *__restrict__ B, CDbl alpha,
                        CDbl beta) {
   __shared__ T Bs[D * D];
   pdl_wait();
   pdl_trigger();
-  for (int64_t ti = blockIdx.x; ti < ntasks; ti += gridDim.x) {
+  // a contiguous range of tasks per CTA: consecutive tasks mostly share their block, so op(B)
+  // is staged again only when the block changes; the row of op(A) is requested before that
+  const int64_t per = (ntasks + gridDim.x - 1) / gridDim.x;
+  const int64_t t_begin = (int64_t)blockIdx.x * per;
+  const int64_t t_end = min(ntasks, t_begin + per);
+  int staged = -1;  // block whose op(B) is in Bs
+  for (int64_t ti = t_begin; ti < t_end; ++ti) {
     const GTile tk = tasks[ti];
     const GBlock b = blocks[tk.block];
     const int n = (int)b.n, k = (int)b.k;
-    __syncthreads();
-    // op(B)(l, j), zero outside k × n (the row loop below runs over the full D × D)
-    for (int e = threadIdx.x; e < D * D; e += blockDim.x) {
-      const int l = e % D, j = e / D;
-      const int64_t idx = (b.opB == TKB_OP_N) ? b.offB + l + (int64_t)j * b.ldb : b.offB + j + (int64_t)l * b.ldb;
-      Bs[e] = (l < k && j < n && tk.kind == 0) ? ldA<T>(B + idx, b.opB == TKB_OP_C) : zero(T{});
-    }
-    __syncthreads();
     const int64_t i = tk.m0 + threadIdx.x;
-    if (i >= b.m) continue;
+    const bool valid = i < b.m;
     // the whole row of op(A) (and of C when β ≠ 0) is fetched before any arithmetic
     // (k, n ≤ D), so the loads of a thread are all in flight together
     const int kk = tk.kind == 0 ? k : 0;
@@ -408,17 +406,29 @@ __global__ void __launch_bounds__(kSkinnyRows)
     T *pc = C + b.offC + i;
     T a[D];
 #pragma unroll
-    for (int l = 0; l < D; ++l) a[l] = (l < kk) ? ldA<T>(pa + l * sa_l, conjA) : zero(T{});
+    for (int l = 0; l < D; ++l) a[l] = (valid && l < kk) ? ldA<T>(pa + l * sa_l, conjA) : zero(T{});
     T acc[D];
     if constexpr (BZ) {
 #pragma unroll
       for (int j = 0; j < D; ++j) acc[j] = zero(T{});
     } else {
 #pragma unroll
-      for (int j = 0; j < D; ++j) acc[j] = (j < n) ? pc[(int64_t)j * b.ldc] : zero(T{});
+      for (int j = 0; j < D; ++j) acc[j] = (valid && j < n) ? pc[(int64_t)j * b.ldc] : zero(T{});
 #pragma unroll
       for (int j = 0; j < D; ++j) acc[j] = mac(acc[j], make_beta<T>(beta), zero(T{}));
     }
+    if (tk.block != staged) {  // uniform over the CTA
+      __syncthreads();
+      // op(B)(l, j), zero outside k × n (the row loop below runs over the full D × D)
+      for (int e = threadIdx.x; e < D * D; e += blockDim.x) {
+        const int l = e % D, j = e / D;
+        const int64_t idx = (b.opB == TKB_OP_N) ? b.offB + l + (int64_t)j * b.ldb : b.offB + j + (int64_t)l * b.ldb;
+        Bs[e] = (l < k && j < n && tk.kind == 0) ? ldA<T>(B + idx, b.opB == TKB_OP_C) : zero(T{});
+      }
+      __syncthreads();
+      staged = tk.block;
+    }
+    if (!valid) continue;
     // acc += (α·a_l)·op(B)_lj
 #pragma unroll
     for (int l = 0; l < D; ++l) {
