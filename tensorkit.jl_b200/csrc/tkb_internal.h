@@ -88,8 +88,9 @@ struct TaskRec {
   int64_t sA, sB, dA, dB;    // strides of the tile dims on both sides
   double u;                  // recoupling coefficient
   int32_t na, nb;            // valid extents of the tile
-  int32_t ta, tb;            // tile extents (powers of two)
-  int32_t mode, pad;
+  int32_t ta, tb;            // tile extents (powers of two; row tiles: ta = na, tb = nb)
+  int32_t mode;              // 0: same fastest dim on both sides, 1: transpose
+  uint32_t mul;              // row tiles: ⌊(2³²−1)/na⌋ + 1, so e / na = umulhi(e, mul) for e < 2¹⁶
 };
 
 struct tkb_table {
@@ -110,6 +111,10 @@ struct tkb_table {
   int32_t *task_group = nullptr;  // ntasks: the group of every task
   int32_t *task_idx = nullptr;    // ntasks × (2 + TKB_MAX_IND): tile coordinates, outer index
   TaskRec *task_rec = nullptr;    // single-tree tables: per-task bases and extents
+  // single-tree tables whose groups all keep their fastest dim (mode 0): exact row tiles
+  // (na = the fast extent, not rounded to a power of two) for the register row-copy kernel
+  int64_t nrow_tasks = 0;
+  TaskRec *row_rec = nullptr;
 };
 
 int tkb_transform_launch(tkb_ctx *ctx, const tkb_table *t, int dtype, void *dst,

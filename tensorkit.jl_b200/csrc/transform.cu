@@ -340,10 +340,74 @@ __global__ void __launch_bounds__(kThreads)
   cp_async_wait<0>();
 }
 
-// TKB_TRANSFORM_KERNEL=plain selects the non-pipelined kernel for every table (comparison)
+// ---- row-copy kernel for single-tree tables whose groups all keep their fastest dim -------
+// Such a transform is a batch of strided row copies (a U(1) or SU(2) permute that leaves the
+// leading leg in place: every sub-block row is contiguous on both sides). Tiles are exact
+// (na × nb, na the full row up to the tile target), so no lane idles on a power-of-two
+// round-up, and nothing is staged: each thread issues kBatch loads, then the kBatch scaled
+// stores, and the next task's loads follow at once. Row and column come from one multiply-high
+// by the precomputed reciprocal `mul` (exact for tile indices below 2¹⁶: Granlund–Montgomery
+// division by invariant integers). Without shared-memory tiles the kernel runs at the
+// occupancy its registers allow, which keeps enough loads in flight per SM for HBM.
+template <typename T, bool CONJ, typename OFF>
+__global__ void __launch_bounds__(kThreads, sizeof(T) == 8 ? 6 : 4)
+    treetransform_rows_kernel(const TaskRec *__restrict__ recs, int64_t ntasks, T *__restrict__ dst,
+                              const T *__restrict__ src, CDbl alpha_, CDbl beta_, int beta_zero) {
+  __shared__ TaskRec rs[kRecCache];
+  const T alpha = scalar_from<T>(alpha_);
+  const T beta = scalar_from<T>(beta_);
+  const bool bz = beta_zero != 0;
+  pdl_trigger();  // the next kernel may be scheduled; it waits for this grid before reading
+  const int64_t per = (ntasks + gridDim.x - 1) / gridDim.x;  // ≤ kRecCache (host)
+  const int64_t t_begin = (int64_t)blockIdx.x * per;
+  const int64_t t_end = min(ntasks, t_begin + per);
+  {
+    const int nw = (int)(t_end > t_begin ? t_end - t_begin : 0) * (int)(sizeof(TaskRec) / 8);
+    const int64_t *srcw = reinterpret_cast<const int64_t *>(recs + t_begin);
+    int64_t *dstw = reinterpret_cast<int64_t *>(rs);
+    for (int i = threadIdx.x; i < nw; i += kThreads) dstw[i] = __ldg(srcw + i);
+  }
+  __syncthreads();
+  pdl_wait();  // the records are static; source and destination belong to earlier kernels
+
+  for (int64_t task = t_begin; task < t_end; ++task) {
+    const TaskRec &R = rs[task - t_begin];
+    const int na = R.na, nel = R.na * R.nb;
+    const uint32_t mul = R.mul;
+    const OFF sA = (OFF)R.sA, sB = (OFF)R.sB, dA = (OFF)R.dA, dB = (OFF)R.dB;
+    const double u = R.u;
+    const T *sb = src + R.sbase;
+    T *db = dst + R.dbase;
+    for (int e0 = 0; e0 < nel; e0 += kThreads * kBatch) {
+      T v[kBatch];
+#pragma unroll
+      for (int q = 0; q < kBatch; ++q) {
+        const int e = e0 + q * kThreads + threadIdx.x;
+        const int row = mul ? (int)__umulhi((unsigned)e, mul) : e, col = e - row * na;
+        if (e < nel) v[q] = ld_val(sb + (OFF)col * sA + (OFF)row * sB, CONJ);
+      }
+#pragma unroll
+      for (int q = 0; q < kBatch; ++q) {
+        const int e = e0 + q * kThreads + threadIdx.x;
+        const int row = mul ? (int)__umulhi((unsigned)e, mul) : e, col = e - row * na;
+        if (e < nel) {
+          T *dp = db + (OFF)col * dA + (OFF)row * dB;
+          *dp = finish(axpy_r(u, v[q], zero_val(T{})), alpha, beta, dp, bz);
+        }
+      }
+    }
+  }
+}
+
+// TKB_TRANSFORM_KERNEL selects a kernel for comparison: "plain" the non-pipelined kernel for
+// every table, "pipe" the staged ring for every single-tree table (no row-copy kernel)
 bool use_plain_transform() {
   const char *e = std::getenv("TKB_TRANSFORM_KERNEL");
   return e && std::strcmp(e, "plain") == 0;
+}
+bool use_pipe_transform() {
+  const char *e = std::getenv("TKB_TRANSFORM_KERNEL");
+  return e && std::strcmp(e, "pipe") == 0;
 }
 
 // CTAs per SM of a pipelined transform kernel: the shared-memory attribute is set and the
@@ -396,7 +460,8 @@ extern "C" int tkb_table_create(tkb_ctx *ctx, const tkb_table_desc *d, tkb_table
   std::vector<int32_t> htask;  // task → group
   std::vector<int32_t> hidx;   // task → (tile a, tile b, outer multi-index)
   std::vector<TaskRec> hrec;   // task → tree-0 bases and extents (single-tree tables)
-  bool all_off32 = true;
+  std::vector<TaskRec> hrow;   // exact row tiles (single-tree tables, every group mode 0)
+  bool all_off32 = true, all_rows = true, row_off32 = true;
   std::vector<double> hcoef;
   int64_t ntasks = 0, er = 0, ew = 0;
   size_t smem_max_f64 = 0, smem_max_c128 = 0;
@@ -617,9 +682,54 @@ extern "C" int tkb_table_create(tkb_ctx *ctx, const tkb_table_desc *d, tkb_table
         rec.ta = (int32_t)ta;
         rec.tb = (int32_t)tb;
         rec.mode = tg.mode;
-        rec.pad = 0;
+        rec.mul = 0;
         hrec.push_back(rec);
       }
+    }
+    if (nsrc == 1 && ndst == 1 && tg.mode == 0 && all_rows) {
+      // exact row tiles: ra elements of the fast dim (the whole row up to the tile target)
+      // times rb rows of the largest other dim; a fastest, then b, then the outer dims
+      const int64_t L = dims[fa].size, LB = db >= 0 ? dims[db].size : 1;
+      const int64_t ra = std::min<int64_t>(L, kTileElems);
+      const int64_t rb = std::max<int64_t>(1, std::min<int64_t>(LB, kTileElems / ra));
+      const int64_t nra = (L + ra - 1) / ra, nrb = (LB + rb - 1) / rb;
+      {
+        const int64_t lim = (int64_t)INT32_MAX;
+        const int64_t so = (ra - 1) * tg.sa0 + (rb - 1) * tg.sb0, dso = (ra - 1) * tg.da0 + (rb - 1) * tg.db0;
+        if (tg.sa0 > lim || tg.sb0 > lim || tg.da0 > lim || tg.db0 > lim || so > lim || dso > lim) row_off32 = false;
+      }
+      for (int64_t o = 0; o < nouter_total; ++o) {
+        int64_t r = o, sbo = d->src_offsets[s0], dbo = d->dst_offsets[t0];
+        for (int q = 0; q < tg.nouter; ++q) {
+          const Dim &dq = dims[tg.outer[q]];
+          const int64_t i = r % dq.size;
+          r /= dq.size;
+          sbo += i * dq.ss[0];
+          dbo += i * dq.ds[0];
+        }
+        for (int64_t ib = 0; ib < nrb; ++ib) {
+          for (int64_t ia = 0; ia < nra; ++ia) {
+            const int64_t a0 = ia * ra, b0 = ib * rb;
+            TaskRec rec;
+            rec.sbase = sbo + a0 * tg.sa0 + b0 * tg.sb0;
+            rec.dbase = dbo + a0 * tg.da0 + b0 * tg.db0;
+            rec.na = (int32_t)std::min<int64_t>(ra, L - a0);
+            rec.nb = (int32_t)std::min<int64_t>(rb, LB - b0);
+            rec.sA = tg.sa0;
+            rec.sB = tg.sb0;
+            rec.dA = tg.da0;
+            rec.dB = tg.db0;
+            rec.u = tg.u0;
+            rec.ta = rec.na;
+            rec.tb = rec.nb;
+            rec.mode = 0;
+            rec.mul = rec.na > 1 ? 0xFFFFFFFFu / (uint32_t)rec.na + 1u : 0u;
+            hrow.push_back(rec);
+          }
+        }
+      }
+    } else {
+      all_rows = false;
     }
     hg.push_back(tg);
   }
@@ -635,6 +745,7 @@ extern "C" int tkb_table_create(tkb_ctx *ctx, const tkb_table_desc *d, tkb_table
   t->max_trees = max_trees;
   t->single_tree = max_trees == 1 && max_dst == 1;
   t->off32 = all_off32;
+  if (t->single_tree && all_rows && row_off32) t->nrow_tasks = (int64_t)hrow.size();
   t->smem_f64 = smem_max_f64;
   t->smem_c128 = smem_max_c128;
   t->src_len = d->src_len;
@@ -650,6 +761,8 @@ extern "C" int tkb_table_create(tkb_ctx *ctx, const tkb_table_desc *d, tkb_table
   if (e == cudaSuccess) e = up((void **)&t->task_group, htask.data(), htask.size() * 4);
   if (e == cudaSuccess) e = up((void **)&t->task_idx, hidx.data(), hidx.size() * 4);
   if (e == cudaSuccess && t->single_tree) e = up((void **)&t->task_rec, hrec.data(), hrec.size() * sizeof(TaskRec));
+  if (e == cudaSuccess && t->nrow_tasks > 0)
+    e = up((void **)&t->row_rec, hrow.data(), hrow.size() * sizeof(TaskRec));
   if (e == cudaSuccess) e = up((void **)&t->sstr, hsstr.data(), hsstr.size() * 8);
   if (e == cudaSuccess) e = up((void **)&t->soff, hsoff.data(), hsoff.size() * 8);
   if (e == cudaSuccess) e = up((void **)&t->dstr, hdstr.data(), hdstr.size() * 8);
@@ -670,6 +783,7 @@ extern "C" int tkb_table_destroy(tkb_table *t) {
   cudaFree(t->task_group);
   cudaFree(t->task_idx);
   cudaFree(t->task_rec);
+  cudaFree(t->row_rec);
   cudaFree(t->sstr);
   cudaFree(t->soff);
   cudaFree(t->dstr);
@@ -693,6 +807,38 @@ int tkb_transform_launch(tkb_ctx *ctx, const tkb_table *t, int dtype, void *dst,
   const int grid = (int)std::min<int64_t>(t->ntasks, (int64_t)ctx->num_sms * 16);
   CDbl a{alpha.re, alpha.im}, b{beta.re, beta.im};
   const int bz = (beta.re == 0.0 && beta.im == 0.0) ? 1 : 0;
+  if (t->nrow_tasks > 0 && (dtype == TKB_F64 || dtype == TKB_C128) && !use_plain_transform() &&
+      !use_pipe_transform()) {
+    if (dtype == TKB_F64 && (alpha.im != 0.0 || beta.im != 0.0))
+      return tkb_set_error(ctx, TKB_ERR_ARG, "complex scalar with real data");
+    // persistent CTAs: as many as reside at once, with at most kRecCache tasks each
+    using KD = void (*)(const TaskRec *, int64_t, double *, const double *, CDbl, CDbl, int);
+    using KC = void (*)(const TaskRec *, int64_t, double2 *, const double2 *, CDbl, CDbl, int);
+    KD kd = nullptr;
+    KC kc = nullptr;
+    const void *kfn;
+    if (dtype == TKB_F64) {
+      kd = treetransform_rows_kernel<double, false, int32_t>;
+      kfn = (const void *)kd;
+    } else {
+      kc = conj ? treetransform_rows_kernel<double2, true, int32_t> : treetransform_rows_kernel<double2, false, int32_t>;
+      kfn = (const void *)kc;
+    }
+    const int per_sm = pipe_occupancy(ctx->device, kfn, 0);
+    if (per_sm <= 0) return tkb_set_error(ctx, TKB_ERR_CUDA, "row transform: occupancy query failed");
+    const int64_t nt = t->nrow_tasks;
+    int64_t pg = std::min<int64_t>(nt, (int64_t)ctx->num_sms * per_sm);
+    pg = std::max<int64_t>(pg, (nt + kRecCache - 1) / kRecCache);
+    if (kd)
+      TKB_CUDA_TRY(ctx, launch_pdl(kd, dim3((int)pg), dim3(kThreads), 0, ctx->stream, t->row_rec, nt,
+                                   (double *)dst, (const double *)src, a, b, bz));
+    else
+      TKB_CUDA_TRY(ctx, launch_pdl(kc, dim3((int)pg), dim3(kThreads), 0, ctx->stream, t->row_rec, nt,
+                                   (double2 *)dst, (const double2 *)src, a, b, bz));
+    ctx->launches++;
+    TKB_CUDA_TRY(ctx, cudaGetLastError());
+    return TKB_OK;
+  }
   if (t->single_tree && (dtype == TKB_F64 || dtype == TKB_C128) && !use_plain_transform()) {
     if (dtype == TKB_F64 && (alpha.im != 0.0 || beta.im != 0.0))
       return tkb_set_error(ctx, TKB_ERR_ARG, "complex scalar with real data");
