@@ -340,9 +340,10 @@ __global__ void __launch_bounds__(kThreads)
   cp_async_wait<0>();
 }
 
-// ---- row-copy kernel for single-tree tables whose groups all keep their fastest dim -------
+// ---- row-copy kernel for single-tree tables whose groups keep their fastest dim ----------
 // Such a transform is a batch of strided row copies (a U(1) or SU(2) permute that leaves the
-// leading leg in place: every sub-block row is contiguous on both sides). Tiles are exact
+// leading leg in place: every sub-block row is contiguous on both sides; a small remainder of
+// transpose groups rides along with uncoalesced reads). Tiles are exact
 // (na × nb, na the full row up to the tile target), so no lane idles on a power-of-two
 // round-up, and nothing is staged: each thread issues kBatch loads, then the kBatch scaled
 // stores, and the next task's loads follow at once. Row and column come from one multiply-high
@@ -462,6 +463,7 @@ extern "C" int tkb_table_create(tkb_ctx *ctx, const tkb_table_desc *d, tkb_table
   std::vector<TaskRec> hrec;   // task → tree-0 bases and extents (single-tree tables)
   std::vector<TaskRec> hrow;   // exact row tiles (single-tree tables, every group mode 0)
   bool all_off32 = true, all_rows = true, row_off32 = true;
+  int64_t row_transposed = 0;  // elements of transpose groups in the row tiles
   std::vector<double> hcoef;
   int64_t ntasks = 0, er = 0, ew = 0;
   size_t smem_max_f64 = 0, smem_max_c128 = 0;
@@ -686,9 +688,11 @@ extern "C" int tkb_table_create(tkb_ctx *ctx, const tkb_table_desc *d, tkb_table
         hrec.push_back(rec);
       }
     }
-    if (nsrc == 1 && ndst == 1 && tg.mode == 0 && all_rows) {
-      // exact row tiles: ra elements of the fast dim (the whole row up to the tile target)
-      // times rb rows of the largest other dim; a fastest, then b, then the outer dims
+    if (nsrc == 1 && ndst == 1 && all_rows) {
+      // exact row tiles: ra elements of the destination's fast dim (the whole row up to the
+      // tile target) times rb rows of the tile's b dim (the largest other dim; for a transpose
+      // group the source's fast dim, read uncoalesced); a fastest, then b, then the outer dims
+      if (tg.mode == 1) row_transposed += vol;
       const int64_t L = dims[fa].size, LB = db >= 0 ? dims[db].size : 1;
       const int64_t ra = std::min<int64_t>(L, kTileElems);
       const int64_t rb = std::max<int64_t>(1, std::min<int64_t>(LB, kTileElems / ra));
@@ -745,7 +749,9 @@ extern "C" int tkb_table_create(tkb_ctx *ctx, const tkb_table_desc *d, tkb_table
   t->max_trees = max_trees;
   t->single_tree = max_trees == 1 && max_dst == 1;
   t->off32 = all_off32;
-  if (t->single_tree && all_rows && row_off32) t->nrow_tasks = (int64_t)hrow.size();
+  // the row kernel takes the table when its transpose groups are a small remainder (sub-blocks
+  // whose leading leg has dimension 1, for example); otherwise the staged ring transposes
+  if (t->single_tree && all_rows && row_off32 && row_transposed * 64 <= er) t->nrow_tasks = (int64_t)hrow.size();
   t->smem_f64 = smem_max_f64;
   t->smem_c128 = smem_max_c128;
   t->src_len = d->src_len;

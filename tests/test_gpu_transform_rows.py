@@ -6,8 +6,8 @@ row tiles. The same call through the staged ring (TKB_TRANSFORM_KERNEL=pipe) and
 kernel (=plain) does the same arithmetic per element, α·(u·v) + β·d, so the results must agree
 bit for bit; the oracle checks them to 1e-12 (FP64). Cases: rows longer than one tile (split
 into chunks), sub-blocks of one element (scalar rows), α/β accumulation, complex data and a
-lazy-adjoint source (conjugating loads), and a permute that moves the leading leg (transpose
-groups, which keep the staged kernel)."""
+lazy-adjoint source (conjugating loads), a few small transpose groups among the row groups, and
+a permute that moves the leading leg (transpose groups throughout, which keep the staged kernel)."""
 import numpy as np
 import pytest
 import torch
@@ -21,7 +21,8 @@ KERNELS = ("", "pipe", "plain")
 
 
 def _long_rows():
-    V = O.Space({U1(0): 2600, U1(1): 37, U1(-1): 300})
+    # the dimension-1 sector makes a few transpose groups (its leading leg is squeezed away)
+    V = O.Space({U1(0): 2600, U1(1): 37, U1(-1): 300, U1(2): 1})
     Pp = O.Space({U1(0): 1, U1(1): 1})
     return O.Hom([V, Pp, Pp], [V])
 
