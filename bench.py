@@ -403,28 +403,51 @@ def kernel_roofline(args, log, ctx, flush):
     stream = ctx.stream
     reps = max(args.steps, 10)
     rows = []
+    sink = torch.zeros(1, dtype=torch.int64, device=flush.device)
+
+    def timed(fn, clean=False):
+        # mean device time of `fn` after a 256 MB write flush; clean: the flush buffer is then
+        # read back, so L2 holds clean unrelated lines and no write-back of the flush lands in `fn`
+        evs = []
+        for _ in range(reps):
+            flush.zero_()
+            if clean:
+                sink.copy_(flush.view(torch.int64).sum().view(1))
+            a = torch.cuda.Event(enable_timing=True)
+            b = torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            fn()
+            b.record(stream)
+            evs.append((a, b))
+        stream.synchronize()
+        return statistics.mean(x.elapsed_time(y) for x, y in evs)
+
     with torch.cuda.stream(stream):
         for e in log:
             for _ in range(3):
                 relaunch(e)
             stream.synchronize()
-            evs = []
-            for _ in range(reps):
-                flush.zero_()
-                a = torch.cuda.Event(enable_timing=True)
-                b = torch.cuda.Event(enable_timing=True)
-                a.record(stream)
-                relaunch(e)
-                b.record(stream)
-                evs.append((a, b))
-            stream.synchronize()
-            ms = statistics.mean(x.elapsed_time(y) for x, y in evs)
+            ms = timed(lambda: relaunch(e))
             if e[0] == "transform":
                 t = e[1]
                 el = e[2].data.element_size()
                 nbytes = el * (t.elems_read + t.elems_written * (1 if e[5] == 0 else 2))
-                rows.append({"kernel": "treetransform", "ms": ms, "bytes": nbytes,
-                             "gbs": nbytes / (ms * 1e-3) / 1e9, "frac_hbm": nbytes / (ms * 1e-3) / 1e9 / hbm})
+                row = {"kernel": "treetransform", "ms": ms, "bytes": nbytes,
+                       "gbs": nbytes / (ms * 1e-3) / 1e9, "frac_hbm": nbytes / (ms * 1e-3) / 1e9 / hbm}
+                if nbytes >= (64 << 20):
+                    # the same launch after a clean flush, and a device-to-device copy of the same
+                    # bytes (half read, half written) under both flushes: what HBM gives at this size
+                    ms_c = timed(lambda: relaunch(e), clean=True)
+                    half = nbytes // 2
+                    csrc = torch.empty(half, dtype=torch.uint8, device=flush.device)
+                    cdst = torch.empty_like(csrc)
+                    cp = timed(lambda: cdst.copy_(csrc))
+                    cp_c = timed(lambda: cdst.copy_(csrc), clean=True)
+                    del csrc, cdst
+                    row.update({"ms_clean_l2": ms_c, "frac_hbm_clean_l2": nbytes / (ms_c * 1e-3) / 1e9 / hbm,
+                                "memcpy_ms": cp, "memcpy_ms_clean_l2": cp_c,
+                                "of_memcpy": cp / ms, "of_memcpy_clean_l2": cp_c / ms_c})
+                rows.append(row)
             else:
                 plan = e[1]
                 S = plan.slices
