@@ -226,7 +226,7 @@ int tkb_gemm_plan_create(tkb_ctx *ctx, const tkb_gemm_desc *d, tkb_plan **out) {
     p->hblocks.push_back(b);
     if (b.m > 0 && b.n > 0) {
       if (b.skinny) {
-        for (int64_t m0 = 0; m0 < b.m; m0 += kSkinnyRows)
+        for (int64_t m0 = 0; m0 < b.m; m0 += kSkinnyTaskRows)
           sk.push_back({(int32_t)i, (int32_t)m0, 0, b.k > 0 ? 0 : 1});
       } else {
         for (int64_t m0 = 0; m0 < b.m; m0 += 64)

@@ -375,51 +375,46 @@ __device__ __forceinline__ double2 scl(double2 v, CDbl a) {
   return make_double2(a.x * v.x - a.y * v.y, a.x * v.y + a.y * v.x);
 }
 
-// D bounds n and k of every block of the launch (4, 8 or 16): the row loops are unrolled to D,
-// so the code stays small for the common narrow bonds.
+// D bounds n and k of every block of the launch (2, 4, 6, 8 or 16) and R rows are handled per
+// thread and pass: the R·k loads of op(A) of a pass are all issued before any arithmetic, so a
+// thread keeps up to R·k loads in flight (R·D ≈ 16 values in registers, half that for complex
+// data). Rows of a task: kSkinnyTaskRows, in passes of kSkinnyRows·R. Per element the arithmetic
+// is acc = β·c (or 0), then acc = fma(α·a_l, op(B)_lj, acc) for l = 0 … k−1; rows where a_l was
+// not loaded (invalid rows, l ≥ k) hold zeros and are not stored.
+// resident CTAs asked of the register allocator: the real β = 0 passes of widths 2 and 6 fit
+// 48 registers (5 CTAs per SM), the other widths up to 8 fit 80 (3 CTAs), width 16 fits 128
 template <typename T, bool BZ, int D>
-__global__ void __launch_bounds__(kSkinnyRows, (sizeof(T) == 8 && D <= 8 && BZ) ? 4 : 1)
+constexpr int kSkinnyMinCtas = (sizeof(T) == 8 && BZ && (D == 2 || D == 6)) ? 5 : D <= 8 ? 3 : 2;
+
+template <typename T, bool BZ, int D, int R>
+__global__ void __launch_bounds__(kSkinnyRows, kSkinnyMinCtas<T, BZ, D>)
     gemm_skinny_kernel(const GBlock *__restrict__ blocks, const GTile *__restrict__ tasks, int64_t ntasks,
                        T *__restrict__ C, const T *__restrict__ A, const T *__restrict__ B, CDbl alpha,
                        CDbl beta) {
+  static_assert(kSkinnyTaskRows % (kSkinnyRows * R) == 0, "a task is a whole number of passes");
   __shared__ T Bs[D * D];
+  // a contiguous, even share of the tasks per CTA: consecutive tasks mostly share their block,
+  // so op(B) is staged again only when the block changes
+  const int64_t t_begin = (int64_t)blockIdx.x * ntasks / gridDim.x;
+  const int64_t t_end = (int64_t)(blockIdx.x + 1) * ntasks / gridDim.x;
   pdl_wait();
   pdl_trigger();
-  // a contiguous range of tasks per CTA: consecutive tasks mostly share their block, so op(B)
-  // is staged again only when the block changes; the row of op(A) is requested before that
-  const int64_t per = (ntasks + gridDim.x - 1) / gridDim.x;
-  const int64_t t_begin = (int64_t)blockIdx.x * per;
-  const int64_t t_end = min(ntasks, t_begin + per);
   int staged = -1;  // block whose op(B) is in Bs
   for (int64_t ti = t_begin; ti < t_end; ++ti) {
     const GTile tk = tasks[ti];
-    const GBlock b = blocks[tk.block];
+    const GBlock &b = blocks[tk.block];
     const int n = (int)b.n, k = (int)b.k;
-    const int64_t i = tk.m0 + threadIdx.x;
-    const bool valid = i < b.m;
-    // the whole row of op(A) (and of C when β ≠ 0) is fetched before any arithmetic
-    // (k, n ≤ D), so the loads of a thread are all in flight together
+    const int64_t m = b.m;
     const int kk = tk.kind == 0 ? k : 0;
     const bool conjA = b.opA == TKB_OP_C;
     const int64_t sa_l = (b.opA == TKB_OP_N) ? b.lda : 1;
-    const T *pa = A + ((b.opA == TKB_OP_N) ? b.offA + i : b.offA + i * b.lda);
-    T *pc = C + b.offC + i;
-    T a[D];
-#pragma unroll
-    for (int l = 0; l < D; ++l) a[l] = (valid && l < kk) ? ldA<T>(pa + l * sa_l, conjA) : zero(T{});
-    T acc[D];
-    if constexpr (BZ) {
-#pragma unroll
-      for (int j = 0; j < D; ++j) acc[j] = zero(T{});
-    } else {
-#pragma unroll
-      for (int j = 0; j < D; ++j) acc[j] = (valid && j < n) ? pc[(int64_t)j * b.ldc] : zero(T{});
-#pragma unroll
-      for (int j = 0; j < D; ++j) acc[j] = mac(acc[j], make_beta<T>(beta), zero(T{}));
-    }
+    const int64_t sa_i = (b.opA == TKB_OP_N) ? 1 : b.lda;
+    const int64_t ldc = b.ldc;
+    const T *pa0 = A + b.offA;
+    T *pc0 = C + b.offC;
     if (tk.block != staged) {  // uniform over the CTA
       __syncthreads();
-      // op(B)(l, j), zero outside k × n (the row loop below runs over the full D × D)
+      // op(B)(l, j), zero outside k × n (the row loops below run over the full D × D)
       for (int e = threadIdx.x; e < D * D; e += blockDim.x) {
         const int l = e % D, j = e / D;
         const int64_t idx = (b.opB == TKB_OP_N) ? b.offB + l + (int64_t)j * b.ldb : b.offB + j + (int64_t)l * b.ldb;
@@ -428,21 +423,78 @@ __global__ void __launch_bounds__(kSkinnyRows, (sizeof(T) == 8 && D <= 8 && BZ) 
       __syncthreads();
       staged = tk.block;
     }
-    if (!valid) continue;
-    // acc += (α·a_l)·op(B)_lj
+    for (int p0 = 0; p0 < kSkinnyTaskRows; p0 += kSkinnyRows * R) {
+      int64_t row[R];
+      bool valid[R];
+      T a[R][D];
 #pragma unroll
-    for (int l = 0; l < D; ++l) {
-      if (l < kk) {
-        const T al = scl(a[l], alpha);
+      for (int r = 0; r < R; ++r) {
+        row[r] = tk.m0 + p0 + r * kSkinnyRows + threadIdx.x;
+        valid[r] = row[r] < m;
+      }
 #pragma unroll
-        for (int j = 0; j < D; ++j)
-          if (j < n) acc[j] = mac(al, Bs[l + j * D], acc[j]);
+      for (int r = 0; r < R; ++r)
+#pragma unroll
+        for (int l = 0; l < D; ++l)
+          a[r][l] = (valid[r] && l < kk) ? ldA<T>(pa0 + row[r] * sa_i + l * sa_l, conjA) : zero(T{});
+      // α·a once per element of op(A); each op(B)_lj is read from shared memory once per pass
+      // and used for the R rows
+#pragma unroll
+      for (int r = 0; r < R; ++r)
+#pragma unroll
+        for (int l = 0; l < D; ++l) a[r][l] = scl(a[r][l], alpha);
+#pragma unroll
+      for (int j = 0; j < D; ++j) {
+        if (j < n) {
+          T acc[R];
+#pragma unroll
+          for (int r = 0; r < R; ++r) {
+            acc[r] = zero(T{});
+            if constexpr (!BZ)
+              if (valid[r]) acc[r] = mac(pc0[row[r] + (int64_t)j * ldc], make_beta<T>(beta), zero(T{}));
+          }
+#pragma unroll
+          for (int l = 0; l < D; ++l) {
+            if (l < kk) {
+              const T bl = Bs[l + j * D];
+#pragma unroll
+              for (int r = 0; r < R; ++r) acc[r] = mac(a[r][l], bl, acc[r]);
+            }
+          }
+#pragma unroll
+          for (int r = 0; r < R; ++r)
+            if (valid[r]) pc0[row[r] + (int64_t)j * ldc] = acc[r];
+        }
       }
     }
-#pragma unroll
-    for (int j = 0; j < D; ++j)
-      if (j < n) pc[(int64_t)j * b.ldc] = acc[j];
   }
+}
+
+}  // namespace
+
+namespace {
+
+template <typename T, bool BZ, int D>
+int skinny_launch_t(tkb_ctx *ctx, const tkb_plan *p, T *C, const T *A, const T *B, CDbl a, CDbl bb) {
+  // R·D ≈ 16 values of op(A) per thread (complex: 8)
+  constexpr int R = sizeof(T) == 8 ? (D <= 4 ? 4 : D <= 8 ? 2 : 1) : (D <= 2 ? 4 : D <= 4 ? 2 : 1);
+  auto k = gemm_skinny_kernel<T, BZ, D, R>;
+  const int per_sm = tkb_occupancy(ctx->device, (const void *)k, kSkinnyRows, 0);
+  if (per_sm <= 0) return tkb_set_error(ctx, TKB_ERR_CUDA, "skinny GEMM: occupancy query failed");
+  const int grid = (int)std::min<int64_t>(p->nsk, (int64_t)ctx->num_sms * per_sm);
+  TKB_CUDA_TRY(ctx, launch_pdl(k, dim3(grid), dim3(kSkinnyRows), 0, ctx->stream, p->blocks, p->sktasks, p->nsk, C,
+                               A, B, a, bb));
+  return TKB_OK;
+}
+
+template <typename T, bool BZ>
+int skinny_launch_d(tkb_ctx *ctx, const tkb_plan *p, T *C, const T *A, const T *B, CDbl a, CDbl bb) {
+  const int d = p->sk_dim;
+  if (d <= 2) return skinny_launch_t<T, BZ, 2>(ctx, p, C, A, B, a, bb);
+  if (d <= 4) return skinny_launch_t<T, BZ, 4>(ctx, p, C, A, B, a, bb);
+  if (d <= 6) return skinny_launch_t<T, BZ, 6>(ctx, p, C, A, B, a, bb);
+  if (d <= 8) return skinny_launch_t<T, BZ, 8>(ctx, p, C, A, B, a, bb);
+  return skinny_launch_t<T, BZ, 16>(ctx, p, C, A, B, a, bb);
 }
 
 }  // namespace
@@ -450,29 +502,16 @@ __global__ void __launch_bounds__(kSkinnyRows, (sizeof(T) == 8 && D <= 8 && BZ) 
 int tkb_gemm_skinny_launch(tkb_ctx *ctx, const tkb_plan *p, void *C, const void *A,
                            const void *B, tkb_scalar alpha, tkb_scalar beta) {
   if (p->nsk == 0) return TKB_OK;
-  const int grid = (int)std::min<int64_t>(p->nsk, (int64_t)ctx->num_sms * 8);
   const CDbl a{alpha.re, alpha.im}, bb{beta.re, beta.im};
   const bool bz = beta.re == 0.0 && beta.im == 0.0;
-  const int dsel = p->sk_dim <= 4 ? 0 : p->sk_dim <= 8 ? 1 : 2;
-  if (p->dtype == TKB_F64) {
-    using K = void (*)(const GBlock *, const GTile *, int64_t, double *, const double *, const double *, CDbl, CDbl);
-    const K ks[2][3] = {{gemm_skinny_kernel<double, false, 4>, gemm_skinny_kernel<double, false, 8>,
-                         gemm_skinny_kernel<double, false, 16>},
-                        {gemm_skinny_kernel<double, true, 4>, gemm_skinny_kernel<double, true, 8>,
-                         gemm_skinny_kernel<double, true, 16>}};
-    TKB_CUDA_TRY(ctx, launch_pdl(ks[bz][dsel], dim3(grid), dim3(kSkinnyRows), 0, ctx->stream, p->blocks,
-                                 p->sktasks, p->nsk, (double *)C, (const double *)A, (const double *)B, a, bb));
-  } else {
-    using K = void (*)(const GBlock *, const GTile *, int64_t, double2 *, const double2 *, const double2 *, CDbl,
-                       CDbl);
-    const K ks[2][3] = {{gemm_skinny_kernel<double2, false, 4>, gemm_skinny_kernel<double2, false, 8>,
-                         gemm_skinny_kernel<double2, false, 16>},
-                        {gemm_skinny_kernel<double2, true, 4>, gemm_skinny_kernel<double2, true, 8>,
-                         gemm_skinny_kernel<double2, true, 16>}};
-    TKB_CUDA_TRY(ctx, launch_pdl(ks[bz][dsel], dim3(grid), dim3(kSkinnyRows), 0, ctx->stream, p->blocks,
-                                 p->sktasks, p->nsk, (double2 *)C, (const double2 *)A, (const double2 *)B, a,
-                                 bb));
-  }
+  int rc;
+  if (p->dtype == TKB_F64)
+    rc = bz ? skinny_launch_d<double, true>(ctx, p, (double *)C, (const double *)A, (const double *)B, a, bb)
+            : skinny_launch_d<double, false>(ctx, p, (double *)C, (const double *)A, (const double *)B, a, bb);
+  else
+    rc = bz ? skinny_launch_d<double2, true>(ctx, p, (double2 *)C, (const double2 *)A, (const double2 *)B, a, bb)
+            : skinny_launch_d<double2, false>(ctx, p, (double2 *)C, (const double2 *)A, (const double2 *)B, a, bb);
+  if (rc != TKB_OK) return rc;
   ctx->launches++;
   TKB_CUDA_TRY(ctx, cudaGetLastError());
   return TKB_OK;

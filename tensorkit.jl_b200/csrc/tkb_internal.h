@@ -163,7 +163,11 @@ struct GBlock {
 
 constexpr int kSkinnyMax = 16;        // n and k bound of the skinny (row-per-thread) path
 constexpr int kSkinnyMinRows = 2048;  // smaller blocks go to the tiled kernels
-constexpr int kSkinnyRows = 256;
+constexpr int kSkinnyRows = 256;       // threads of a skinny CTA (one row each per pass)
+constexpr int kSkinnyTaskRows = 1024;  // rows of one skinny task
+
+// CTAs per SM of a kernel (cached per kernel and device; sets the dynamic shared memory limit)
+int tkb_occupancy(int device, const void *kfn, int threads, size_t smem);
 
 int tkb_gemm_skinny_launch(tkb_ctx *ctx, const tkb_plan *p, void *C, const void *A,
                            const void *B, tkb_scalar alpha, tkb_scalar beta);
@@ -178,7 +182,7 @@ struct tkb_plan {
   tkb_ctx *owner = nullptr;
   int dtype = 0, precision = 0, slices = 0;
   int64_t nblocks = 0, ntiles = 0;
-  GTile *sktasks = nullptr;     // skinny blocks: (block, first row) tasks of kSkinnyRows rows
+  GTile *sktasks = nullptr;     // skinny blocks: (block, first row) tasks of kSkinnyTaskRows rows
   int64_t nsk = 0;
   int sk_dim = 0;               // max(n, k) over the skinny blocks
   double flops = 0;

@@ -411,10 +411,18 @@ bool use_pipe_transform() {
   return e && std::strcmp(e, "pipe") == 0;
 }
 
-// CTAs per SM of a pipelined transform kernel: the shared-memory attribute is set and the
-// occupancy queried once per kernel (the shared memory size is fixed per element type), so
-// eager launches make no attribute calls (per device: attributes belong to the device's context)
-int pipe_occupancy(int device, const void *kfn, size_t smem) {
+int64_t pow2ceil(int64_t x) {
+  int64_t p = 1;
+  while (p < x) p <<= 1;
+  return p;
+}
+
+}  // namespace
+
+// CTAs per SM of a kernel launched with `threads` threads and `smem` bytes of dynamic shared
+// memory: the shared-memory attribute is set and the occupancy queried once per kernel and
+// device (each kernel has one launch shape), so eager launches make no attribute calls
+int tkb_occupancy(int device, const void *kfn, int threads, size_t smem) {
   static std::mutex mu;
   static std::unordered_map<const void *, int> cache[64];
   if (device < 0 || device >= 64) return 0;
@@ -423,18 +431,10 @@ int pipe_occupancy(int device, const void *kfn, size_t smem) {
   if (it != cache[device].end()) return it->second;
   if (cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) return 0;
   int per_sm = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kfn, kThreads, smem) != cudaSuccess) return 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kfn, threads, smem) != cudaSuccess) return 0;
   cache[device][kfn] = per_sm;
   return per_sm;
 }
-
-int64_t pow2ceil(int64_t x) {
-  int64_t p = 1;
-  while (p < x) p <<= 1;
-  return p;
-}
-
-}  // namespace
 
 extern "C" int tkb_table_create(tkb_ctx *ctx, const tkb_table_desc *d, tkb_table **out) {
   if (!ctx || !d || !out) return TKB_ERR_ARG;
@@ -830,7 +830,7 @@ int tkb_transform_launch(tkb_ctx *ctx, const tkb_table *t, int dtype, void *dst,
       kc = conj ? treetransform_rows_kernel<double2, true, int32_t> : treetransform_rows_kernel<double2, false, int32_t>;
       kfn = (const void *)kc;
     }
-    const int per_sm = pipe_occupancy(ctx->device, kfn, 0);
+    const int per_sm = tkb_occupancy(ctx->device, kfn, kThreads, 0);
     if (per_sm <= 0) return tkb_set_error(ctx, TKB_ERR_CUDA, "row transform: occupancy query failed");
     const int64_t nt = t->nrow_tasks;
     int64_t pg = std::min<int64_t>(nt, (int64_t)ctx->num_sms * per_sm);
@@ -867,7 +867,7 @@ int tkb_transform_launch(tkb_ctx *ctx, const tkb_table *t, int dtype, void *dst,
                             : treetransform_pipe_kernel<double2, false, int64_t>);
       kfn = (const void *)kc;
     }
-    const int per_sm = pipe_occupancy(ctx->device, kfn, smem);
+    const int per_sm = tkb_occupancy(ctx->device, kfn, kThreads, smem);
     if (per_sm <= 0) return tkb_set_error(ctx, TKB_ERR_CUDA, "pipelined transform: occupancy query failed");
     int64_t pg = std::min<int64_t>(t->ntasks, (int64_t)ctx->num_sms * std::max(1, per_sm));
     pg = std::max<int64_t>(pg, (t->ntasks + kRecCache - 1) / kRecCache);

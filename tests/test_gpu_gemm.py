@@ -131,3 +131,34 @@ def test_split_many_short_k_tasks(cplx):
     C = tk.TensorMap.zeros(to_hom(ref.W), dtype=Ad.dtype, device=Ad.device)
     tk.mul_(C, Ad, tk.AdjointTensorMap(Btd), 1.0, 0.0, prec="split")
     assert relerr(C.to_host(), ref.data) <= TOL_SPLIT
+
+
+def _skinny(kmax, nmax, cplx, adjA):
+    """Tall blocks (≥ 2048 rows) against narrow bonds: every block has n, k ≤ 16, so the
+    plan runs the skinny row kernel; kmax/nmax pick its width class (2, 4, 6, 8, 16)."""
+    V = O.Space({O.U1(0): 3000, O.U1(1): 2500, O.U1(-1): 2100})
+    Wk = O.Space({O.U1(0): kmax, O.U1(1): max(1, kmax - 1), O.U1(-1): 1})
+    Wn = O.Space({O.U1(0): max(1, nmax - 1), O.U1(1): nmax, O.U1(-1): 2 if nmax > 1 else 1})
+    A = O.randn(O.Hom([Wk], [V]) if adjA else O.Hom([V], [Wk]), 31, cplx)
+    B = O.randn(O.Hom([Wk], [Wn]), 32, cplx)
+    return A, B
+
+
+@pytest.mark.parametrize("prec", ["plain", "split"])
+@pytest.mark.parametrize("kn", [(2, 2), (3, 4), (5, 5), (7, 6), (13, 16)], ids=lambda x: f"k{x[0]}n{x[1]}")
+@pytest.mark.parametrize("cplx", [False, True])
+def test_mul_skinny_blocks(prec, kn, cplx):
+    kmax, nmax = kn
+    for adjA in (False, True):
+        A, B = _skinny(kmax, nmax, cplx, adjA)
+        ref0 = O.mul(A, B, adjA=adjA)
+        Ad, Bd = to_device(A), to_device(B)
+        opA = tk.AdjointTensorMap(Ad) if adjA else Ad
+        C = tk.TensorMap.zeros(to_hom(ref0.W), dtype=Ad.dtype, device=Ad.device)
+        tk.mul_(C, opA, Bd, 1.0, 0.0, prec=prec)
+        assert relerr(C.to_host(), ref0.data) <= TOL_PLAIN, adjA
+        C0 = O.randn(ref0.W, 33, cplx)
+        Cd = to_device(C0)
+        alpha, beta = (0.75 + 0.5j, -1.5 + 0.25j) if cplx else (0.75, -1.5)
+        tk.mul_(Cd, opA, Bd, alpha, beta, prec=prec)
+        assert relerr(Cd.to_host(), alpha * ref0.data + beta * C0.data) <= TOL_PLAIN, adjA
