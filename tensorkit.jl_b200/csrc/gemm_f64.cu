@@ -381,6 +381,63 @@ __device__ __forceinline__ double2 scl(double2 v, CDbl a) {
 // data). Rows of a task: kSkinnyTaskRows, in passes of kSkinnyRows·R. Per element the arithmetic
 // is acc = β·c (or 0), then acc = fma(α·a_l, op(B)_lj, acc) for l = 0 … k−1; rows where a_l was
 // not loaded (invalid rows, l ≥ k) hold zeros and are not stored.
+// rows per thread and pass for a width class: ≈ 16 values of op(A) in registers (complex: 8)
+template <typename T, int DK>
+constexpr int kSkinnyRowsPerPass = sizeof(T) == 8 ? (DK <= 4 ? 4 : DK <= 8 ? 2 : 1) : (DK <= 2 ? 4 : DK <= 4 ? 2 : 1);
+
+// One task's rows in passes of kSkinnyRows·RR (rows per thread RR): all RR·k loads of op(A) are
+// issued first; blocks with n, k ≤ DK ≤ D (op(B) staged with leading dimension D)
+template <typename T, bool BZ, int D, int DK, int RR>
+__device__ __forceinline__ void skinny_passes(int64_t m0, int64_t m, int kk, int n, const T *__restrict__ pa0,
+                                              int64_t sa_i, int64_t sa_l, bool conjA, T *__restrict__ pc0,
+                                              int64_t ldc, const T *Bs, CDbl alpha, CDbl beta) {
+  static_assert(kSkinnyTaskRows % (kSkinnyRows * RR) == 0, "a task is a whole number of passes");
+  for (int p0 = 0; p0 < kSkinnyTaskRows; p0 += kSkinnyRows * RR) {
+    int64_t row[RR];
+    bool valid[RR];
+    T a[RR][DK];
+#pragma unroll
+    for (int r = 0; r < RR; ++r) {
+      row[r] = m0 + p0 + r * kSkinnyRows + threadIdx.x;
+      valid[r] = row[r] < m;
+    }
+#pragma unroll
+    for (int r = 0; r < RR; ++r)
+#pragma unroll
+      for (int l = 0; l < DK; ++l)
+        a[r][l] = (valid[r] && l < kk) ? ldA<T>(pa0 + row[r] * sa_i + l * sa_l, conjA) : zero(T{});
+    // α·a once per element of op(A); each op(B)_lj is read from shared memory once per pass
+    // and used for the RR rows
+#pragma unroll
+    for (int r = 0; r < RR; ++r)
+#pragma unroll
+      for (int l = 0; l < DK; ++l) a[r][l] = scl(a[r][l], alpha);
+#pragma unroll
+    for (int j = 0; j < DK; ++j) {
+      if (j < n) {
+        T acc[RR];
+#pragma unroll
+        for (int r = 0; r < RR; ++r) {
+          acc[r] = zero(T{});
+          if constexpr (!BZ)
+            if (valid[r]) acc[r] = mac(pc0[row[r] + (int64_t)j * ldc], make_beta<T>(beta), zero(T{}));
+        }
+#pragma unroll
+        for (int l = 0; l < DK; ++l) {
+          if (l < kk) {
+            const T bl = Bs[l + j * D];
+#pragma unroll
+            for (int r = 0; r < RR; ++r) acc[r] = mac(a[r][l], bl, acc[r]);
+          }
+        }
+#pragma unroll
+        for (int r = 0; r < RR; ++r)
+          if (valid[r]) pc0[row[r] + (int64_t)j * ldc] = acc[r];
+      }
+    }
+  }
+}
+
 // resident CTAs asked of the register allocator: the real β = 0 passes of widths 2 and 6 fit
 // 48 registers (5 CTAs per SM), the other widths up to 8 fit 80 (3 CTAs), width 16 fits 128
 template <typename T, bool BZ, int D>
@@ -391,7 +448,6 @@ __global__ void __launch_bounds__(kSkinnyRows, kSkinnyMinCtas<T, BZ, D>)
     gemm_skinny_kernel(const GBlock *__restrict__ blocks, const GTile *__restrict__ tasks, int64_t ntasks,
                        T *__restrict__ C, const T *__restrict__ A, const T *__restrict__ B, CDbl alpha,
                        CDbl beta) {
-  static_assert(kSkinnyTaskRows % (kSkinnyRows * R) == 0, "a task is a whole number of passes");
   __shared__ T Bs[D * D];
   // a contiguous, even share of the tasks per CTA: consecutive tasks mostly share their block,
   // so op(B) is staged again only when the block changes
@@ -423,50 +479,16 @@ __global__ void __launch_bounds__(kSkinnyRows, kSkinnyMinCtas<T, BZ, D>)
       __syncthreads();
       staged = tk.block;
     }
-    for (int p0 = 0; p0 < kSkinnyTaskRows; p0 += kSkinnyRows * R) {
-      int64_t row[R];
-      bool valid[R];
-      T a[R][D];
-#pragma unroll
-      for (int r = 0; r < R; ++r) {
-        row[r] = tk.m0 + p0 + r * kSkinnyRows + threadIdx.x;
-        valid[r] = row[r] < m;
-      }
-#pragma unroll
-      for (int r = 0; r < R; ++r)
-#pragma unroll
-        for (int l = 0; l < D; ++l)
-          a[r][l] = (valid[r] && l < kk) ? ldA<T>(pa0 + row[r] * sa_i + l * sa_l, conjA) : zero(T{});
-      // α·a once per element of op(A); each op(B)_lj is read from shared memory once per pass
-      // and used for the R rows
-#pragma unroll
-      for (int r = 0; r < R; ++r)
-#pragma unroll
-        for (int l = 0; l < D; ++l) a[r][l] = scl(a[r][l], alpha);
-#pragma unroll
-      for (int j = 0; j < D; ++j) {
-        if (j < n) {
-          T acc[R];
-#pragma unroll
-          for (int r = 0; r < R; ++r) {
-            acc[r] = zero(T{});
-            if constexpr (!BZ)
-              if (valid[r]) acc[r] = mac(pc0[row[r] + (int64_t)j * ldc], make_beta<T>(beta), zero(T{}));
-          }
-#pragma unroll
-          for (int l = 0; l < D; ++l) {
-            if (l < kk) {
-              const T bl = Bs[l + j * D];
-#pragma unroll
-              for (int r = 0; r < R; ++r) acc[r] = mac(a[r][l], bl, acc[r]);
-            }
-          }
-#pragma unroll
-          for (int r = 0; r < R; ++r)
-            if (valid[r]) pc0[row[r] + (int64_t)j * ldc] = acc[r];
-        }
-      }
-    }
+    // blocks narrower than the launch's width class run a narrower pass with more rows per
+    // thread (uniform per task), so their threads also keep ≈ 16 loads in flight
+    if (D > 2 && kk <= 2 && n <= 2)
+      skinny_passes<T, BZ, D, 2, kSkinnyRowsPerPass<T, 2>>(tk.m0, m, kk, n, pa0, sa_i, sa_l, conjA, pc0, ldc, Bs,
+                                                           alpha, beta);
+    else if (D > 4 && kk <= 4 && n <= 4)
+      skinny_passes<T, BZ, D, 4, kSkinnyRowsPerPass<T, 4>>(tk.m0, m, kk, n, pa0, sa_i, sa_l, conjA, pc0, ldc, Bs,
+                                                           alpha, beta);
+    else
+      skinny_passes<T, BZ, D, D, R>(tk.m0, m, kk, n, pa0, sa_i, sa_l, conjA, pc0, ldc, Bs, alpha, beta);
   }
 }
 
@@ -476,9 +498,7 @@ namespace {
 
 template <typename T, bool BZ, int D>
 int skinny_launch_t(tkb_ctx *ctx, const tkb_plan *p, T *C, const T *A, const T *B, CDbl a, CDbl bb) {
-  // R·D ≈ 16 values of op(A) per thread (complex: 8)
-  constexpr int R = sizeof(T) == 8 ? (D <= 4 ? 4 : D <= 8 ? 2 : 1) : (D <= 2 ? 4 : D <= 4 ? 2 : 1);
-  auto k = gemm_skinny_kernel<T, BZ, D, R>;
+  auto k = gemm_skinny_kernel<T, BZ, D, kSkinnyRowsPerPass<T, D>>;
   const int per_sm = tkb_occupancy(ctx->device, (const void *)k, kSkinnyRows, 0);
   if (per_sm <= 0) return tkb_set_error(ctx, TKB_ERR_CUDA, "skinny GEMM: occupancy query failed");
   const int grid = (int)std::min<int64_t>(p->nsk, (int64_t)ctx->num_sms * per_sm);
