@@ -21,10 +21,19 @@ KERNELS = ("", "pipe", "plain")
 
 
 def _long_rows():
-    # the dimension-1 sector makes a few transpose groups (its leading leg is squeezed away)
     V = O.Space({U1(0): 2600, U1(1): 37, U1(-1): 300, U1(2): 1})
     Pp = O.Space({U1(0): 1, U1(1): 1})
     return O.Hom([V, Pp, Pp], [V])
+
+
+def _mixed_transpose():
+    # sub-blocks whose leading sector has dimension 1 lose that leg, and a permute that keeps leg
+    # 1 first but swaps legs 2 and 3 turns them into transpose groups: 30 of 76 030 elements, so
+    # the table still runs as row tiles with those few groups read uncoalesced
+    V = O.Space({U1(0): 2000, U1(1): 1})
+    V2 = O.Space({U1(0): 4, U1(1): 3})
+    V3 = O.Space({U1(0): 5, U1(1): 6, U1(2): 2})
+    return O.Hom([V, V2], [V3])
 
 
 def _scalar_blocks():
@@ -45,7 +54,8 @@ def _run(monkeypatch, kernel, fn):
 @pytest.mark.parametrize("make,perms", [
     (_long_rows, [((1, 3), (2, 4)), ((1,), (4, 2, 3)), ((1, 4, 2), (3,)), ((4, 1), (2, 3))]),
     (_scalar_blocks, [((1, 3, 2), (5, 4)), ((1,), (2, 3, 4, 5)), ((3, 1, 2, 5), (4,))]),
-], ids=["long_rows", "scalar_blocks"])
+    (_mixed_transpose, [((1, 3), (2,)), ((1,), (3, 2)), ((3, 1), (2,))]),
+], ids=["long_rows", "scalar_blocks", "mixed_transpose"])
 @pytest.mark.parametrize("cplx", [False, True])
 def test_rows_kernel_bitwise_and_oracle(monkeypatch, make, perms, cplx):
     W = make()
