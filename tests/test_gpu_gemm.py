@@ -162,3 +162,22 @@ def test_mul_skinny_blocks(prec, kn, cplx):
         alpha, beta = (0.75 + 0.5j, -1.5 + 0.25j) if cplx else (0.75, -1.5)
         tk.mul_(Cd, opA, Bd, alpha, beta, prec=prec)
         assert relerr(Cd.to_host(), alpha * ref0.data + beta * C0.data) <= TOL_PLAIN, adjA
+
+
+@pytest.mark.parametrize("prec", ["plain", "split"])
+@pytest.mark.parametrize("cplx", [False, True])
+def test_mul_skinny_missing_sector_scales_by_beta(prec, cplx):
+    """A tall narrow sector of C that A·B does not reach (k = 0 on the skinny path) gets β·C_c;
+    the other sectors get α·A_c·B_c + β·C_c (src/tensors/linalg.jl:341-366)."""
+    V = O.Space({O.U1(0): 3000, O.U1(1): 2500, O.U1(2): 2200})
+    Wk = O.Space({O.U1(0): 3, O.U1(1): 2})
+    Wn = O.Space({O.U1(0): 2, O.U1(1): 3, O.U1(2): 4})
+    A = O.randn(O.Hom([V], [Wk]), 41, cplx)
+    B = O.randn(O.Hom([Wk], [Wn]), 42, cplx)
+    C0 = O.randn(O.Hom([V], [Wn]), 43, cplx)
+    ref = O.mul(A, B)
+    assert ref.W == C0.W
+    alpha, beta = (1.25 - 0.5j, 0.5 + 0.75j) if cplx else (1.25, 0.5)
+    Cd = to_device(C0)
+    tk.mul_(Cd, to_device(A), to_device(B), alpha, beta, prec=prec)
+    assert relerr(Cd.to_host(), alpha * ref.data + beta * C0.data) <= TOL_PLAIN
