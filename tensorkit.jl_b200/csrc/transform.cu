@@ -470,7 +470,7 @@ extern "C" int tkb_table_create(tkb_ctx *ctx, const tkb_table_desc *d, tkb_table
   int max_trees = 1, max_dst = 1;
   // tile target: 2048 elements per task, smaller when the whole transform would not give
   // every SM about four tasks (small permutes are latency-bound, not bandwidth-bound)
-  int64_t kTileElems = kTileElemsMax;
+  int64_t kTileElems = kTileElemsMax, kRowTileElems = kTileElemsMax;
   {
     int64_t total = 0;
     for (int64_t g = 0; g < G; ++g) {
@@ -479,6 +479,9 @@ extern "C" int tkb_table_create(tkb_ctx *ctx, const tkb_table_desc *d, tkb_table
       total += vol * (d->group_dst_ptr[g + 1] - d->group_dst_ptr[g]);
     }
     while (kTileElems > 256 && total / kTileElems < (int64_t)ctx->num_sms * 4) kTileElems >>= 1;
+    // row tiles: about two per SM at least; a row task costs a fixed record fetch and one load
+    // round trip, so small transforms run faster with fewer, larger row tasks
+    while (kRowTileElems > 256 && total / kRowTileElems < (int64_t)ctx->num_sms * 2) kRowTileElems >>= 1;
   }
 
   for (int64_t g = 0; g < G; ++g) {
@@ -694,8 +697,8 @@ extern "C" int tkb_table_create(tkb_ctx *ctx, const tkb_table_desc *d, tkb_table
       // group the source's fast dim, read uncoalesced); a fastest, then b, then the outer dims
       if (tg.mode == 1) row_transposed += vol;
       const int64_t L = dims[fa].size, LB = db >= 0 ? dims[db].size : 1;
-      const int64_t ra = std::min<int64_t>(L, kTileElems);
-      const int64_t rb = std::max<int64_t>(1, std::min<int64_t>(LB, kTileElems / ra));
+      const int64_t ra = std::min<int64_t>(L, kRowTileElems);
+      const int64_t rb = std::max<int64_t>(1, std::min<int64_t>(LB, kRowTileElems / ra));
       const int64_t nra = (L + ra - 1) / ra, nrb = (LB + rb - 1) / rb;
       {
         const int64_t lim = (int64_t)INT32_MAX;
