@@ -27,13 +27,29 @@ def sources():
 
 
 def build(force: bool = False, verbose: bool = False) -> str:
+    """Compile every translation unit in parallel (one nvcc per file), then link the .so."""
+    from concurrent.futures import ThreadPoolExecutor
     os.makedirs(LIBDIR, exist_ok=True)
     out = os.path.join(LIBDIR, "libtkb200.so")
     if not force and os.path.exists(out):
         newest = max(os.path.getmtime(s) for s in sources())
         if os.path.getmtime(out) >= newest:
             return out
-    cmd = [nvcc()] + NVCC_FLAGS + ["-o", out] + [os.path.join(CSRC, s) for s in SOURCES]
+    objdir = os.path.join(LIBDIR, "obj")
+    os.makedirs(objdir, exist_ok=True)
+    compile_flags = [f for f in NVCC_FLAGS if f != "-shared"]
+
+    def compile_one(src):
+        obj = os.path.join(objdir, os.path.splitext(src)[0] + ".o")
+        cmd = [nvcc()] + compile_flags + ["-c", os.path.join(CSRC, src), "-o", obj]
+        if verbose:
+            print(" ".join(cmd), file=sys.stderr)
+        subprocess.run(cmd, check=True)
+        return obj
+
+    with ThreadPoolExecutor(max_workers=len(SOURCES)) as ex:
+        objs = list(ex.map(compile_one, SOURCES))
+    cmd = [nvcc()] + NVCC_FLAGS + ["-o", out] + objs
     if verbose:
         print(" ".join(cmd), file=sys.stderr)
     subprocess.run(cmd, check=True)
