@@ -155,7 +155,10 @@ typedef struct tkb_gemm_desc {
   int64_t lenA, lenB, lenC;      /* elements in each data vector (bounds check) */
   int32_t dtype;                 /* tkb_dtype */
   int32_t precision;             /* tkb_precision */
-  int32_t slices;                /* split precision: int8 slices per operand, 0 = auto */
+  int32_t slices;                /* split precision: int8 slices per operand. 0 = auto: up to 7,
+                                    chosen per block on the device, with an FP64 fallback for
+                                    blocks and tiles the slices cannot serve to 1e-12; 3..7 =
+                                    exactly that many for every block, unchecked */
 } tkb_gemm_desc;
 
 int tkb_gemm_plan_create(tkb_ctx *ctx, const tkb_gemm_desc *desc, tkb_plan **out);
@@ -164,6 +167,13 @@ int tkb_gemm_plan_destroy(tkb_plan *plan);
 int tkb_gemm_plan_info(const tkb_plan *plan, double *flops, int32_t *slices);
 int tkb_grouped_gemm(tkb_ctx *ctx, const tkb_plan *plan, void *C, const void *A,
                      const void *B, tkb_scalar alpha, tkb_scalar beta);
+/* Split precision: the slice count each block used in the plan's last tkb_grouped_gemm (with
+ * slices = 0 in the descriptor, chosen on the device from the block's exponents and row norms;
+ * 0 = the block ran in FP64, -1 = no products: k = 0, a skinny block or a plain-precision plan),
+ * in out[0 .. nblocks-1], and in out[nblocks] the number of output tiles whose a-posteriori error
+ * check sent them to FP64. n must be at least nblocks + 1. Waits for the context's stream. (No
+ * reference counterpart: the reference's mul! runs every block in FP64.) */
+int tkb_gemm_plan_slices(tkb_ctx *ctx, const tkb_plan *plan, int32_t *out, int64_t n);
 
 /* ---- weighted block reductions ------------------------------------------------------ */
 /* Segments s: elements x[off_s + i*stride_s], i < count_s, weighted by weight_s (dim(c)).
@@ -190,8 +200,12 @@ int tkb_reduce_async(tkb_ctx *ctx, const tkb_rplan *plan, int kind, int dtype,
  * as tkb_rplan_create) and receives (re, im) in host_out after the stream has completed.
  * Limits: at most 1024 segments (TKB_ERR_SIZE beyond that). The first call on a device
  * looks up the array's device address for that device; make that first call before any
- * stream capture. All calls share the array, so calls that overlap on the GPU (other
- * streams, other host threads) race and must be serialised by the caller. */
+ * stream capture. With CUDA's lazy module loading that first call also loads the library's
+ * kernels onto the device, which can itself need device memory: make it once per device at
+ * start-up (any valid call that reduces at least one element), not first from an
+ * out-of-memory recovery path. Host-side staging uses a few KiB of the caller's stack. All
+ * calls share the array, so calls that overlap on the GPU (other streams, other host threads)
+ * race and must be serialised by the caller. */
 int tkb_reduce_noalloc(int device, void *stream, int kind, int dtype, const void *x,
                        const void *y, int64_t len, int64_t nseg, const int64_t *off,
                        const int64_t *count, const int64_t *stride, const double *weight,

@@ -243,6 +243,7 @@ int tkb_gemm_plan_create(tkb_ctx *ctx, const tkb_gemm_desc *d, tkb_plan **out) {
   p->ntiles = (int64_t)tiles.size();
   int rc = TKB_OK;
   if (d->precision == TKB_SPLIT_INT8) rc = tkb_gemm_split_prepare(ctx, p);
+  else rc = tkb_gemm_plain_prepare(ctx, p, tiles);
   if (rc != TKB_OK) {
     tkb_gemm_plan_destroy(p);
     return rc;
@@ -274,12 +275,14 @@ int tkb_gemm_plan_destroy(tkb_plan *p) {
   cudaFree(p->blocks);
   cudaFree(p->tiles);
   cudaFree(p->sktasks);
+  cudaFree(p->ptasks);
+  cudaFree(p->bstat);
+  cudaFree(p->bslices);
   cudaFree(p->kstiles);
   cudaFree(p->part);
   cudaFree(p->pcnt);
   cudaFree(p->stiles);
   cudaFree(p->sjobs);
-  cudaFree(p->srow_begin);
   delete p;
   return TKB_OK;
 }
@@ -288,6 +291,21 @@ int tkb_gemm_plan_info(const tkb_plan *p, double *flops, int32_t *slices) {
   if (!p) return TKB_ERR_ARG;
   if (flops) *flops = p->flops;
   if (slices) *slices = p->precision == TKB_SPLIT_INT8 ? p->slices : 0;
+  return TKB_OK;
+}
+
+int tkb_gemm_plan_slices(tkb_ctx *ctx, const tkb_plan *p, int32_t *out, int64_t n) {
+  if (!ctx || !p || !out) return tkb_set_error(ctx, TKB_ERR_ARG, "null argument");
+  if (p->owner != ctx) return tkb_set_error(ctx, TKB_ERR_ARG, "plan belongs to another context");
+  const int64_t nb = (int64_t)p->hblocks.size();
+  if (n < nb + 1) return tkb_set_error(ctx, TKB_ERR_ARG, "output array shorter than nblocks + 1");
+  if (!p->bslices) {
+    for (int64_t i = 0; i < nb; ++i) out[i] = -1;
+    out[nb] = 0;
+    return TKB_OK;
+  }
+  TKB_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+  TKB_CUDA_TRY(ctx, cudaMemcpy(out, p->bslices, (size_t)(nb + 1) * sizeof(int32_t), cudaMemcpyDeviceToHost));
   return TKB_OK;
 }
 
@@ -315,7 +333,7 @@ int tkb_rplan_create(tkb_ctx *ctx, int64_t nseg, const int64_t *off, const int64
   for (int64_t s = 0; s < nseg; ++s) {
     if (count[s] < 0 || off[s] < 0 || stride[s] < 0)
       return tkb_set_error(ctx, TKB_ERR_ARG, "invalid segment");
-    if (count[s] > 0 && off[s] + (count[s] - 1) * stride[s] >= len)
+    if (count[s] > 0 && !tkb_segment_in_bounds(off[s], count[s], stride[s], len))
       return tkb_set_error(ctx, TKB_ERR_SIZE, "segment outside the data vector");
     segs[s] = {off[s], count[s], stride[s], weight[s]};
     begin[s + 1] = begin[s] + count[s];

@@ -1,15 +1,23 @@
-// Plain FP64 / ComplexF64 grouped block GEMM: one persistent launch for all coupled-sector
-// blocks of a TensorKit mul! (src/tensors/linalg.jl:330-370), tiles taken from a
-// cost-ordered device work queue (largest k first).
+// Plain FP64 / ComplexF64 grouped block GEMM: one launch for all coupled-sector blocks of a
+// TensorKit mul! (src/tensors/linalg.jl:330-370).
 //
 // Tensor path: FP64 DMMA (mma.sync.m8n8k4.f64). tcgen05 has no f64 kind, so the
 // double-precision tensor pipe is reached through DMMA; the split-precision path
 // (gemm_split.cu) is the tcgen05 one.
 //
-// CTA tile 64x64x16, 4 warps in a 2x2 grid (each 32x32 = 4x4 DMMA tiles), operands
-// double-buffered in shared memory with 8-byte cp.async (zero-filled outside the block,
-// so any lda/offset parity works). Complex blocks keep separate re/im planes and issue
-// four real DMMA per fragment pair.
+// Work decomposition: 64×64 output tiles; when the tiles would leave resident CTA slots idle,
+// the K loops of the longest tiles are cut into pieces (split K) so that the pieces fill about
+// one wave. Tasks (tile, K range) are sorted by decreasing length and dealt round-robin to the
+// CTAs of the launch (a static, cost-ordered queue: no atomics to claim work). A piece of a split
+// tile stores its FP64 partial tile; the piece that arrives last on the tile's counter adds all
+// partials in piece order (deterministic, no piece waits for another) and applies α, β.
+//
+// CTA: 4 warps in a 2×2 grid (each 32×32 = 4×4 DMMA tiles), BK = 16, a three-stage cp.async
+// ring (two stages in flight while one is consumed; one barrier per K step). Operand tiles are
+// copied in 16-byte pairs when the block's layout keeps pairs aligned (op N, even offsets and
+// leading dimensions, 16-byte aligned base), else in 8-byte elements; elements outside the block
+// are zero-filled, so any lda/offset parity works. Complex blocks copy whole 16-byte elements and
+// issue four real DMMA per fragment pair.
 #include <algorithm>
 #include <cstring>
 
@@ -17,11 +25,21 @@
 
 namespace {
 
-constexpr int BM = 64, BN = 64, BK = 16;
-constexpr int APAD = 4, BPAD = 4;
+constexpr int BM = 64, BN = 64, BK = 16, NST = 3;
+constexpr int APAD = 4, BPAD = 4;      // real: keeps 16-byte row alignment, spreads banks
+constexpr int CAPAD = 2, CBPAD = 2;    // complex (16-byte elements)
+constexpr int kRealThreads = 128, kCplxThreads = 256;
 
 struct CDbl {
   double x, y;
+};
+
+// one task of the plain kernels: a 64×64 output tile and a range of its K steps
+struct PTask {
+  int32_t block, m0, n0, kind;  // kind 0: products, 1: β-scale only (k = 0)
+  int32_t kb, ke;               // K steps [kb, ke) of BK
+  int32_t slot, nsplit;         // split K: counter slot, pieces of the tile (1 = unsplit)
+  int32_t sid, pbase;           // piece index, first partial buffer of the tile
 };
 
 __device__ __forceinline__ void cp_async8(void *smem, const void *gmem, bool pred) {
@@ -29,9 +47,14 @@ __device__ __forceinline__ void cp_async8(void *smem, const void *gmem, bool pre
   const int sz = pred ? 8 : 0;
   asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(s), "l"(gmem), "r"(sz));
 }
+// 16-byte copy of which the first `bytes` (0, 8 or 16) come from global memory, the rest zero
+__device__ __forceinline__ void cp_async16(void *smem, const void *gmem, int bytes) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(s), "l"(gmem), "r"(bytes));
+}
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
-__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::); }
-__device__ __forceinline__ void cp_async_wait_1() { asm volatile("cp.async.wait_group 1;\n" ::); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N)); }
 
 __device__ __forceinline__ void dmma(double &c0, double &c1, double a, double b) {
   asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
@@ -41,275 +64,305 @@ __device__ __forceinline__ void dmma(double &c0, double &c1, double a, double b)
 
 // ---- real ----------------------------------------------------------------------------
 struct SmemR {
-  double A[2][BK][BM + APAD];
-  double B[2][BN][BK + BPAD];
+  double A[NST][BK][BM + APAD];  // op(A) tile, [k][row]
+  double B[NST][BN][BK + BPAD];  // op(B) tile, [col][k]
 };
 
-__device__ __forceinline__ void load_tiles_r(SmemR &s, int buf, const GBlock &b, const double *A,
-                                             const double *B, int64_t m0, int64_t n0, int64_t k0) {
+// vec: bit 0 = A tiles as 16-byte pairs, bit 1 = B tiles as 16-byte pairs
+__device__ __forceinline__ void load_tiles_r(SmemR &s, int st, const GBlock &b, const double *A,
+                                             const double *B, int64_t m0, int64_t n0, int64_t k0, int vec) {
   const int tid = threadIdx.x;
-  // A tile: op(A) rows m0.., cols k0..
-  if (b.opA == TKB_OP_N) {
+  if (vec & 1) {  // op N, pairs of rows: 32 pairs × BK columns
 #pragma unroll
-    for (int r = 0; r < (BM * BK) / 128; ++r) {
-      const int e = tid + r * 128;
+    for (int r = 0; r < (BM * BK) / (2 * kRealThreads); ++r) {
+      const int e = tid + r * kRealThreads;
+      const int i2 = e % (BM / 2), l = e / (BM / 2);
+      const int64_t gi = m0 + 2 * i2, gl = k0 + l;
+      const int bytes = (gl < b.k && gi < b.m) ? (gi + 1 < b.m ? 16 : 8) : 0;
+      const double *p = A + b.offA + (bytes ? gi + gl * b.lda : 0);
+      cp_async16(&s.A[st][l][2 * i2], p, bytes);
+    }
+  } else if (b.opA == TKB_OP_N) {
+#pragma unroll
+    for (int r = 0; r < (BM * BK) / kRealThreads; ++r) {
+      const int e = tid + r * kRealThreads;
       const int i = e % BM, l = e / BM;
       const int64_t gi = m0 + i, gl = k0 + l;
       const bool ok = gi < b.m && gl < b.k;
-      const double *p = A + b.offA + (ok ? gi + gl * b.lda : 0);
-      cp_async8(&s.A[buf][l][i], p, ok);
+      cp_async8(&s.A[st][l][i], A + b.offA + (ok ? gi + gl * b.lda : 0), ok);
     }
   } else {
 #pragma unroll
-    for (int r = 0; r < (BM * BK) / 128; ++r) {
-      const int e = tid + r * 128;
+    for (int r = 0; r < (BM * BK) / kRealThreads; ++r) {
+      const int e = tid + r * kRealThreads;
       const int l = e % BK, i = e / BK;
       const int64_t gi = m0 + i, gl = k0 + l;
       const bool ok = gi < b.m && gl < b.k;
-      const double *p = A + b.offA + (ok ? gl + gi * b.lda : 0);
-      cp_async8(&s.A[buf][l][i], p, ok);
+      cp_async8(&s.A[st][l][i], A + b.offA + (ok ? gl + gi * b.lda : 0), ok);
     }
   }
-  if (b.opB == TKB_OP_N) {
+  if (vec & 2) {  // op N, pairs along K: BK/2 pairs × BN columns
 #pragma unroll
-    for (int r = 0; r < (BN * BK) / 128; ++r) {
-      const int e = tid + r * 128;
+    for (int r = 0; r < (BN * BK) / (2 * kRealThreads); ++r) {
+      const int e = tid + r * kRealThreads;
+      const int l2 = e % (BK / 2), j = e / (BK / 2);
+      const int64_t gl = k0 + 2 * l2, gj = n0 + j;
+      const int bytes = (gj < b.n && gl < b.k) ? (gl + 1 < b.k ? 16 : 8) : 0;
+      const double *p = B + b.offB + (bytes ? gl + gj * b.ldb : 0);
+      cp_async16(&s.B[st][j][2 * l2], p, bytes);
+    }
+  } else if (b.opB == TKB_OP_N) {
+#pragma unroll
+    for (int r = 0; r < (BN * BK) / kRealThreads; ++r) {
+      const int e = tid + r * kRealThreads;
       const int l = e % BK, j = e / BK;
       const int64_t gl = k0 + l, gj = n0 + j;
       const bool ok = gl < b.k && gj < b.n;
-      const double *p = B + b.offB + (ok ? gl + gj * b.ldb : 0);
-      cp_async8(&s.B[buf][j][l], p, ok);
+      cp_async8(&s.B[st][j][l], B + b.offB + (ok ? gl + gj * b.ldb : 0), ok);
     }
   } else {
 #pragma unroll
-    for (int r = 0; r < (BN * BK) / 128; ++r) {
-      const int e = tid + r * 128;
+    for (int r = 0; r < (BN * BK) / kRealThreads; ++r) {
+      const int e = tid + r * kRealThreads;
       const int j = e % BN, l = e / BN;
       const int64_t gl = k0 + l, gj = n0 + j;
       const bool ok = gl < b.k && gj < b.n;
-      const double *p = B + b.offB + (ok ? gj + gl * b.ldb : 0);
-      cp_async8(&s.B[buf][j][l], p, ok);
+      cp_async8(&s.B[st][j][l], B + b.offB + (ok ? gj + gl * b.ldb : 0), ok);
     }
   }
 }
 
-__global__ void __launch_bounds__(128)
-    gemm_f64_kernel(const GBlock *__restrict__ blocks, const GTile *__restrict__ tiles, int ntiles,
-                    int *counters, double *__restrict__ C, const double *__restrict__ A,
-                    const double *__restrict__ B, double alpha, double beta) {
-  __shared__ __align__(16) SmemR s;
-  __shared__ int next_tile;
-  pdl_wait();  // operands, output and the work-queue counters belong to earlier kernels too
+// 16-byte pairs are usable for an operand in op N whose offset and leading dimension are even
+// (the base pointer's alignment is checked at launch)
+__device__ __forceinline__ int vec_flags(const GBlock &b, int base_ok) {
+  int v = 0;
+  if ((base_ok & 1) && b.opA == TKB_OP_N && !(b.offA & 1) && !(b.lda & 1)) v |= 1;
+  if ((base_ok & 2) && b.opB == TKB_OP_N && !(b.offB & 1) && !(b.ldb & 1)) v |= 2;
+  return v;
+}
+
+// K loop of one task through the NST-stage ring: `load(st, k0)` fills ring slot st with the
+// tiles at K offset k0, `step(st)` consumes slot st. Every iteration commits one group (possibly
+// empty), so wait_group<NST-2> always means "the group of this iteration's stage has landed".
+template <typename Load, typename Step>
+__device__ __forceinline__ void k_loop(int kb, int ke, Load &&load, Step &&step) {
+  const int nk = ke - kb;
+#pragma unroll
+  for (int st = 0; st < NST - 1; ++st) {
+    if (st < nk) load(st, (int64_t)(kb + st) * BK);
+    cp_async_commit();
+  }
+  for (int kt = 0; kt < nk; ++kt) {
+    cp_async_wait<NST - 2>();
+    __syncthreads();  // stage kt visible to all; every warp is done with stage kt-1's slot
+    const int nxt = kt + NST - 1;
+    if (nxt < nk) load(nxt % NST, (int64_t)(kb + nxt) * BK);
+    cp_async_commit();
+    step(kt % NST);
+  }
+  cp_async_wait<0>();
+  __syncthreads();  // the ring may be refilled by the next task
+}
+
+// Split-K: store this piece's values (q-major: value q of every thread, so warps store
+// contiguous runs), count the arrival; the last piece of the tile reads all partials in piece
+// order and returns true with their sum in v. Unsplit tiles return true with v unchanged.
+template <int NV, int NT>
+__device__ __forceinline__ bool splitk_reduce(const PTask &t, double (&v)[NV], double *part, int *pcnt,
+                                              int *ticket) {
+  if (t.nsplit <= 1) return true;
+  const int tid = threadIdx.x;
+  double *mine = part + (int64_t)(t.pbase + t.sid) * (NV * NT);
+#pragma unroll
+  for (int q = 0; q < NV; ++q) __stcg(&mine[q * NT + tid], v[q]);
+  __threadfence();
+  __syncthreads();
+  if (tid == 0) *ticket = atomicAdd(&pcnt[t.slot], 1);
+  __syncthreads();
+  const bool last = *ticket == t.nsplit - 1;
+  __syncthreads();  // ticket is rewritten by the next task
+  if (!last) return false;
+  __threadfence();
+#pragma unroll
+  for (int q = 0; q < NV; ++q) v[q] = 0.0;
+  for (int sp = 0; sp < t.nsplit; ++sp) {  // piece order: deterministic sum
+    const double *src = part + (int64_t)(t.pbase + sp) * (NV * NT);
+#pragma unroll
+    for (int q = 0; q < NV; ++q) v[q] += __ldcg(&src[q * NT + tid]);
+  }
+  if (tid == 0) pcnt[t.slot] = 0;  // every piece has arrived: the counter is free for the next launch
+  return true;
+}
+
+__global__ void __launch_bounds__(kRealThreads, 3)
+    gemm_f64_kernel(const GBlock *__restrict__ blocks, const PTask *__restrict__ tasks, int ntasks,
+                    double *__restrict__ C, const double *__restrict__ A, const double *__restrict__ B,
+                    double alpha, double beta, double *__restrict__ part, int *__restrict__ pcnt, int base_ok) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  SmemR &s = *reinterpret_cast<SmemR *>(smem_raw);
+  __shared__ int ticket;
+  pdl_wait();  // operands, output and the split-K counters belong to earlier kernels too
   pdl_trigger();
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int wm = warp & 1, wn = warp >> 1;
   const int g = lane >> 2, t = lane & 3;
-  while (true) {
-    if (threadIdx.x == 0) next_tile = atomicAdd(&counters[0], 1);
-    __syncthreads();
-    const int ti = next_tile;
-    __syncthreads();
-    if (ti >= ntiles) break;
-    const GTile tile = tiles[ti];
-    const GBlock b = blocks[tile.block];
-    const int64_t m0 = tile.m0, n0 = tile.n0;
-    double acc[4][4][2];
+  for (int ti = blockIdx.x; ti < ntasks; ti += gridDim.x) {
+    const PTask task = tasks[ti];
+    const GBlock b = blocks[task.block];
+    const int64_t m0 = task.m0, n0 = task.n0;
+    const int vec = vec_flags(b, base_ok);
+    double acc[32];
 #pragma unroll
-    for (int mi = 0; mi < 4; ++mi)
+    for (int q = 0; q < 32; ++q) acc[q] = 0.0;
+    if (task.kind == 0 && task.ke > task.kb) {
+      k_loop(task.kb, task.ke,
+             [&](int st, int64_t k0) { load_tiles_r(s, st, b, A, B, m0, n0, k0, vec); },
+             [&](int st) {
 #pragma unroll
-      for (int ni = 0; ni < 4; ++ni) acc[mi][ni][0] = acc[mi][ni][1] = 0.0;
-    const int64_t nk = (b.k + BK - 1) / BK;
-    if (nk > 0) {
-      load_tiles_r(s, 0, b, A, B, m0, n0, 0);
-      cp_async_commit();
-      for (int64_t kt = 0; kt < nk; ++kt) {
-        const int buf = kt & 1;
-        if (kt + 1 < nk) {
-          load_tiles_r(s, buf ^ 1, b, A, B, m0, n0, (kt + 1) * BK);
-          cp_async_commit();
-          cp_async_wait_1();
-        } else {
-          cp_async_wait_all();
-        }
-        __syncthreads();
+               for (int kk = 0; kk < BK; kk += 4) {
+                 double af[4], bf[4];
 #pragma unroll
-        for (int kk = 0; kk < BK; kk += 4) {
-          double af[4], bf[4];
+                 for (int mi = 0; mi < 4; ++mi) af[mi] = s.A[st][kk + t][wm * 32 + mi * 8 + g];
 #pragma unroll
-          for (int mi = 0; mi < 4; ++mi) af[mi] = s.A[buf][kk + t][wm * 32 + mi * 8 + g];
+                 for (int ni = 0; ni < 4; ++ni) bf[ni] = s.B[st][wn * 32 + ni * 8 + g][kk + t];
 #pragma unroll
-          for (int ni = 0; ni < 4; ++ni) bf[ni] = s.B[buf][wn * 32 + ni * 8 + g][kk + t];
+                 for (int mi = 0; mi < 4; ++mi)
 #pragma unroll
-          for (int mi = 0; mi < 4; ++mi)
-#pragma unroll
-            for (int ni = 0; ni < 4; ++ni) dmma(acc[mi][ni][0], acc[mi][ni][1], af[mi], bf[ni]);
-        }
-        __syncthreads();
-      }
+                   for (int ni = 0; ni < 4; ++ni) dmma(acc[(mi * 4 + ni) * 2], acc[(mi * 4 + ni) * 2 + 1], af[mi], bf[ni]);
+               }
+             });
     }
-    // epilogue: C = α·acc + β·C
+    if (!splitk_reduce<32, kRealThreads>(task, acc, part, pcnt, &ticket)) continue;
+    // epilogue: C = α·acc + β·C, in four row groups (the old values of a group are loaded before
+    // its first store)
 #pragma unroll
     for (int mi = 0; mi < 4; ++mi) {
       const int64_t i = m0 + wm * 32 + mi * 8 + g;
-      if (i >= b.m) continue;
+      double old[8];
 #pragma unroll
-      for (int ni = 0; ni < 4; ++ni) {
+      for (int q = 0; q < 8; ++q) {
+        const int64_t j = n0 + wn * 32 + (q / 2) * 8 + 2 * t + (q % 2);
+        old[q] = (beta != 0.0 && i < b.m && j < b.n) ? C[b.offC + i + j * b.ldc] : 0.0;
+      }
 #pragma unroll
-        for (int h = 0; h < 2; ++h) {
-          const int64_t j = n0 + wn * 32 + ni * 8 + 2 * t + h;
-          if (j >= b.n) continue;
-          double *p = C + b.offC + i + j * b.ldc;
-          double r = alpha * acc[mi][ni][h];
-          if (beta != 0.0) r = fma(beta, *p, r);
-          *p = r;
+      for (int q = 0; q < 8; ++q) {
+        const int64_t j = n0 + wn * 32 + (q / 2) * 8 + 2 * t + (q % 2);
+        if (i < b.m && j < b.n) {
+          double r = alpha * acc[mi * 8 + q];
+          if (beta != 0.0) r = fma(beta, old[q], r);
+          C[b.offC + i + j * b.ldc] = r;
         }
       }
-    }
-  }
-  // self-resetting queue: the last CTA out zeroes the counters for the next launch
-  if (threadIdx.x == 0) {
-    __threadfence();
-    const int done = atomicAdd(&counters[1], 1);
-    if (done == (int)gridDim.x - 1) {
-      atomicExch(&counters[0], 0);
-      atomicExch(&counters[1], 0);
-      __threadfence();
     }
   }
 }
 
 // ---- complex ---------------------------------------------------------------------------
 struct SmemC {
-  double Ar[2][BK][BM + APAD];
-  double Ai[2][BK][BM + APAD];
-  double Br[2][BN][BK + BPAD];
-  double Bi[2][BN][BK + BPAD];
+  double2 A[NST][BK][BM + CAPAD];  // op(A) tile, [k][row], whole complex elements
+  double2 B[NST][BN][BK + CBPAD];  // op(B) tile, [col][k]
 };
 
-__device__ __forceinline__ void load_tiles_c(SmemC &s, int buf, const GBlock &b, const double2 *A,
+__device__ __forceinline__ void load_tiles_c(SmemC &s, int st, const GBlock &b, const double2 *A,
                                              const double2 *B, int64_t m0, int64_t n0, int64_t k0) {
-  const int tid = threadIdx.x;  // 256 threads
-  const double *Ad = reinterpret_cast<const double *>(A);
-  const double *Bd = reinterpret_cast<const double *>(B);
+  const int tid = threadIdx.x;
   if (b.opA == TKB_OP_N) {
 #pragma unroll
-    for (int r = 0; r < (BM * BK) / 256; ++r) {
-      const int e = tid + r * 256;
+    for (int r = 0; r < (BM * BK) / kCplxThreads; ++r) {
+      const int e = tid + r * kCplxThreads;
       const int i = e % BM, l = e / BM;
       const int64_t gi = m0 + i, gl = k0 + l;
       const bool ok = gi < b.m && gl < b.k;
-      const int64_t idx = ok ? b.offA + gi + gl * b.lda : 0;
-      cp_async8(&s.Ar[buf][l][i], Ad + 2 * idx, ok);
-      cp_async8(&s.Ai[buf][l][i], Ad + 2 * idx + 1, ok);
+      cp_async16(&s.A[st][l][i], A + b.offA + (ok ? gi + gl * b.lda : 0), ok ? 16 : 0);
     }
   } else {
 #pragma unroll
-    for (int r = 0; r < (BM * BK) / 256; ++r) {
-      const int e = tid + r * 256;
+    for (int r = 0; r < (BM * BK) / kCplxThreads; ++r) {
+      const int e = tid + r * kCplxThreads;
       const int l = e % BK, i = e / BK;
       const int64_t gi = m0 + i, gl = k0 + l;
       const bool ok = gi < b.m && gl < b.k;
-      const int64_t idx = ok ? b.offA + gl + gi * b.lda : 0;
-      cp_async8(&s.Ar[buf][l][i], Ad + 2 * idx, ok);
-      cp_async8(&s.Ai[buf][l][i], Ad + 2 * idx + 1, ok);
+      cp_async16(&s.A[st][l][i], A + b.offA + (ok ? gl + gi * b.lda : 0), ok ? 16 : 0);
     }
   }
   if (b.opB == TKB_OP_N) {
 #pragma unroll
-    for (int r = 0; r < (BN * BK) / 256; ++r) {
-      const int e = tid + r * 256;
+    for (int r = 0; r < (BN * BK) / kCplxThreads; ++r) {
+      const int e = tid + r * kCplxThreads;
       const int l = e % BK, j = e / BK;
       const int64_t gl = k0 + l, gj = n0 + j;
       const bool ok = gl < b.k && gj < b.n;
-      const int64_t idx = ok ? b.offB + gl + gj * b.ldb : 0;
-      cp_async8(&s.Br[buf][j][l], Bd + 2 * idx, ok);
-      cp_async8(&s.Bi[buf][j][l], Bd + 2 * idx + 1, ok);
+      cp_async16(&s.B[st][j][l], B + b.offB + (ok ? gl + gj * b.ldb : 0), ok ? 16 : 0);
     }
   } else {
 #pragma unroll
-    for (int r = 0; r < (BN * BK) / 256; ++r) {
-      const int e = tid + r * 256;
+    for (int r = 0; r < (BN * BK) / kCplxThreads; ++r) {
+      const int e = tid + r * kCplxThreads;
       const int j = e % BN, l = e / BN;
       const int64_t gl = k0 + l, gj = n0 + j;
       const bool ok = gl < b.k && gj < b.n;
-      const int64_t idx = ok ? b.offB + gj + gl * b.ldb : 0;
-      cp_async8(&s.Br[buf][j][l], Bd + 2 * idx, ok);
-      cp_async8(&s.Bi[buf][j][l], Bd + 2 * idx + 1, ok);
+      cp_async16(&s.B[st][j][l], B + b.offB + (ok ? gj + gl * b.ldb : 0), ok ? 16 : 0);
     }
   }
 }
 
-__global__ void __launch_bounds__(256)
-    gemm_c128_kernel(const GBlock *__restrict__ blocks, const GTile *__restrict__ tiles, int ntiles,
-                     int *counters, double2 *__restrict__ C, const double2 *__restrict__ A,
-                     const double2 *__restrict__ B, CDbl alpha, CDbl beta) {
+__global__ void __launch_bounds__(kCplxThreads, 2)
+    gemm_c128_kernel(const GBlock *__restrict__ blocks, const PTask *__restrict__ tasks, int ntasks,
+                     double2 *__restrict__ C, const double2 *__restrict__ A, const double2 *__restrict__ B,
+                     CDbl alpha, CDbl beta, double *__restrict__ part, int *__restrict__ pcnt) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   SmemC &s = *reinterpret_cast<SmemC *>(smem_raw);
-  __shared__ int next_tile;
+  __shared__ int ticket;
   pdl_wait();
   pdl_trigger();
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;  // 8 warps: 2 (m) x 4 (n)
   const int wm = warp & 1, wn = warp >> 1;                      // warp tile 32 x 16
   const int g = lane >> 2, t = lane & 3;
   const bool bz = beta.x == 0.0 && beta.y == 0.0;
-  while (true) {
-    if (threadIdx.x == 0) next_tile = atomicAdd(&counters[0], 1);
-    __syncthreads();
-    const int ti = next_tile;
-    __syncthreads();
-    if (ti >= ntiles) break;
-    const GTile tile = tiles[ti];
-    const GBlock b = blocks[tile.block];
-    // conjugation of an operand flips the sign of its imaginary plane
+  for (int ti = blockIdx.x; ti < ntasks; ti += gridDim.x) {
+    const PTask task = tasks[ti];
+    const GBlock b = blocks[task.block];
+    // conjugation of an operand flips the sign of its imaginary part
     const double sa = (b.opA == TKB_OP_C) ? -1.0 : 1.0;
     const double sb = (b.opB == TKB_OP_C) ? -1.0 : 1.0;
-    const int64_t m0 = tile.m0, n0 = tile.n0;
-    double ar[4][2][2], ai[4][2][2];
+    const int64_t m0 = task.m0, n0 = task.n0;
+    // acc[(mi*2 + ni)*4 + {0,1}] = Re (columns 2t, 2t+1), +{2,3} = Im
+    double acc[32];
 #pragma unroll
-    for (int mi = 0; mi < 4; ++mi)
+    for (int q = 0; q < 32; ++q) acc[q] = 0.0;
+    if (task.kind == 0 && task.ke > task.kb) {
+      k_loop(task.kb, task.ke, [&](int st, int64_t k0) { load_tiles_c(s, st, b, A, B, m0, n0, k0); },
+             [&](int st) {
 #pragma unroll
-      for (int ni = 0; ni < 2; ++ni) ar[mi][ni][0] = ar[mi][ni][1] = ai[mi][ni][0] = ai[mi][ni][1] = 0.0;
-    const int64_t nk = (b.k + BK - 1) / BK;
-    if (nk > 0) {
-      load_tiles_c(s, 0, b, A, B, m0, n0, 0);
-      cp_async_commit();
-      for (int64_t kt = 0; kt < nk; ++kt) {
-        const int buf = kt & 1;
-        if (kt + 1 < nk) {
-          load_tiles_c(s, buf ^ 1, b, A, B, m0, n0, (kt + 1) * BK);
-          cp_async_commit();
-          cp_async_wait_1();
-        } else {
-          cp_async_wait_all();
-        }
-        __syncthreads();
+               for (int kk = 0; kk < BK; kk += 4) {
+                 double fr[4], fi[4], fin[4], gr[2], gi[2];
 #pragma unroll
-        for (int kk = 0; kk < BK; kk += 4) {
-          double fr[4], fi[4], fin[4], gr[2], gi[2];
+                 for (int mi = 0; mi < 4; ++mi) {
+                   const double2 v = s.A[st][kk + t][wm * 32 + mi * 8 + g];
+                   fr[mi] = v.x;
+                   fi[mi] = sa * v.y;
+                   fin[mi] = -fi[mi];
+                 }
 #pragma unroll
-          for (int mi = 0; mi < 4; ++mi) {
-            fr[mi] = s.Ar[buf][kk + t][wm * 32 + mi * 8 + g];
-            fi[mi] = sa * s.Ai[buf][kk + t][wm * 32 + mi * 8 + g];
-            fin[mi] = -fi[mi];
-          }
+                 for (int ni = 0; ni < 2; ++ni) {
+                   const double2 v = s.B[st][wn * 16 + ni * 8 + g][kk + t];
+                   gr[ni] = v.x;
+                   gi[ni] = sb * v.y;
+                 }
 #pragma unroll
-          for (int ni = 0; ni < 2; ++ni) {
-            gr[ni] = s.Br[buf][wn * 16 + ni * 8 + g][kk + t];
-            gi[ni] = sb * s.Bi[buf][wn * 16 + ni * 8 + g][kk + t];
-          }
+                 for (int mi = 0; mi < 4; ++mi)
 #pragma unroll
-          for (int mi = 0; mi < 4; ++mi)
-#pragma unroll
-            for (int ni = 0; ni < 2; ++ni) {
-              dmma(ar[mi][ni][0], ar[mi][ni][1], fr[mi], gr[ni]);
-              dmma(ar[mi][ni][0], ar[mi][ni][1], fin[mi], gi[ni]);
-              dmma(ai[mi][ni][0], ai[mi][ni][1], fr[mi], gi[ni]);
-              dmma(ai[mi][ni][0], ai[mi][ni][1], fi[mi], gr[ni]);
-            }
-        }
-        __syncthreads();
-      }
+                   for (int ni = 0; ni < 2; ++ni) {
+                     double *a = &acc[(mi * 2 + ni) * 4];
+                     dmma(a[0], a[1], fr[mi], gr[ni]);
+                     dmma(a[0], a[1], fin[mi], gi[ni]);
+                     dmma(a[2], a[3], fr[mi], gi[ni]);
+                     dmma(a[2], a[3], fi[mi], gr[ni]);
+                   }
+               }
+             });
     }
+    if (!splitk_reduce<32, kCplxThreads>(task, acc, part, pcnt, &ticket)) continue;
 #pragma unroll
     for (int mi = 0; mi < 4; ++mi) {
       const int64_t i = m0 + wm * 32 + mi * 8 + g;
@@ -321,7 +374,7 @@ __global__ void __launch_bounds__(256)
           const int64_t j = n0 + wn * 16 + ni * 8 + 2 * t + h;
           if (j >= b.n) continue;
           double2 *p = C + b.offC + i + j * b.ldc;
-          const double vr = ar[mi][ni][h], vi = ai[mi][ni][h];
+          const double vr = acc[(mi * 2 + ni) * 4 + h], vi = acc[(mi * 2 + ni) * 4 + 2 + h];
           double rr = alpha.x * vr - alpha.y * vi;
           double ri = alpha.x * vi + alpha.y * vr;
           if (!bz) {
@@ -332,15 +385,6 @@ __global__ void __launch_bounds__(256)
           *p = make_double2(rr, ri);
         }
       }
-    }
-  }
-  if (threadIdx.x == 0) {
-    __threadfence();
-    const int done = atomicAdd(&counters[1], 1);
-    if (done == (int)gridDim.x - 1) {
-      atomicExch(&counters[0], 0);
-      atomicExch(&counters[1], 0);
-      __threadfence();
     }
   }
 }
@@ -537,24 +581,97 @@ int tkb_gemm_skinny_launch(tkb_ctx *ctx, const tkb_plan *p, void *C, const void 
   return TKB_OK;
 }
 
+namespace {
+constexpr int kMinPieceSteps = 4;  // K steps of BK per split-K piece, at least
+constexpr int kMaxPieces = 8;      // pieces per tile, at most
+}  // namespace
+
+int tkb_gemm_plain_prepare(tkb_ctx *ctx, tkb_plan *p, const std::vector<GTile> &tiles) {
+  const bool cplx = p->dtype == TKB_C128;
+  const void *kfn = cplx ? (const void *)gemm_c128_kernel : (const void *)gemm_f64_kernel;
+  const int threads = cplx ? kCplxThreads : kRealThreads;
+  const size_t smem = cplx ? sizeof(SmemC) : sizeof(SmemR);
+  const int per_sm = tkb_occupancy(ctx->device, kfn, threads, smem);
+  if (per_sm <= 0) return tkb_set_error(ctx, TKB_ERR_CUDA, "plain GEMM: occupancy query failed");
+  const int64_t slots = (int64_t)ctx->num_sms * per_sm;
+  const int64_t nt = (int64_t)tiles.size();
+  int64_t total = 0, maxnk = 1;
+  std::vector<int64_t> nks(nt);
+  for (int64_t i = 0; i < nt; ++i) {
+    const GTile &t = tiles[i];
+    nks[i] = t.kind == 0 ? (p->hblocks[t.block].k + BK - 1) / BK : 0;
+    total += nks[i];
+    maxnk = std::max(maxnk, nks[i]);
+  }
+  auto pieces = [&](int64_t nk, int64_t target) {
+    return (int)std::min<int64_t>(kMaxPieces, std::max<int64_t>(1, (nk + target - 1) / target));
+  };
+  // the shortest piece length (at least kMinPieceSteps) whose tasks still fit the resident slots
+  int64_t target = maxnk;
+  if (nt < slots) {
+    target = std::max<int64_t>(kMinPieceSteps, (total + slots - 1) / slots);
+    for (; target < maxnk; ++target) {
+      int64_t cnt = 0;
+      for (int64_t i = 0; i < nt; ++i) cnt += pieces(nks[i], target);
+      if (cnt <= slots) break;
+    }
+  }
+  std::vector<PTask> tasks;
+  int nslots = 0, npart = 0;
+  for (int64_t i = 0; i < nt; ++i) {
+    const GTile &t = tiles[i];
+    const int nk = (int)nks[i];
+    const int ks = t.kind == 0 ? pieces(nk, target) : 1;
+    if (ks == 1) {
+      tasks.push_back({t.block, t.m0, t.n0, t.kind, 0, nk, -1, 1, 0, 0});
+    } else {
+      const int slot = nslots++;
+      for (int s = 0; s < ks; ++s)
+        tasks.push_back({t.block, t.m0, t.n0, t.kind, s * nk / ks, (s + 1) * nk / ks, slot, ks, s, npart});
+      npart += ks;
+    }
+  }
+  // longest first; CTA b takes tasks b, b + grid, ... (a static cost-ordered queue)
+  std::stable_sort(tasks.begin(), tasks.end(),
+                   [](const PTask &x, const PTask &y) { return (x.ke - x.kb) > (y.ke - y.kb); });
+  p->nptasks = (int64_t)tasks.size();
+  p->pgrid = (int)std::min<int64_t>(p->nptasks, slots);
+  cudaError_t e = cudaSuccess;
+  if (!tasks.empty()) {
+    e = cudaMalloc(&p->ptasks, tasks.size() * sizeof(PTask));
+    if (e == cudaSuccess) e = cudaMemcpy(p->ptasks, tasks.data(), tasks.size() * sizeof(PTask), cudaMemcpyHostToDevice);
+  }
+  if (e == cudaSuccess && nslots > 0) {
+    e = cudaMalloc((void **)&p->part, (size_t)npart * 32 * threads * sizeof(double));
+    if (e == cudaSuccess) e = cudaMalloc((void **)&p->pcnt, nslots * sizeof(int));
+    if (e == cudaSuccess) e = cudaMemset(p->pcnt, 0, nslots * sizeof(int));
+  }
+  if (e != cudaSuccess)
+    return tkb_set_error(ctx, TKB_ERR_CUDA, std::string("plain plan upload: ") + cudaGetErrorString(e));
+  return TKB_OK;
+}
+
 int tkb_gemm_launch(tkb_ctx *ctx, const tkb_plan *p, void *C, const void *A, const void *B,
                     tkb_scalar alpha, tkb_scalar beta) {
-  if (p->ntiles == 0) return TKB_OK;
+  if (p->nptasks == 0) return TKB_OK;
   if (p->dtype == TKB_F64) {
     if (alpha.im != 0.0 || beta.im != 0.0)
       return tkb_set_error(ctx, TKB_ERR_ARG, "complex scalar with real data");
-    const int grid = (int)std::min<int64_t>(p->ntiles, (int64_t)ctx->num_sms * 4);
-    TKB_CUDA_TRY(ctx, launch_pdl(gemm_f64_kernel, dim3(grid), dim3(128), 0, ctx->stream, p->blocks, p->tiles,
-                                 (int)p->ntiles, ctx->counters, (double *)C, (const double *)A,
-                                 (const double *)B, alpha.re, beta.re));
+    const size_t smem = sizeof(SmemR);
+    TKB_CUDA_TRY(ctx, cudaFuncSetAttribute(gemm_f64_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    const int base_ok = (((uintptr_t)A & 15) == 0 ? 1 : 0) | (((uintptr_t)B & 15) == 0 ? 2 : 0);
+    TKB_CUDA_TRY(ctx, launch_pdl(gemm_f64_kernel, dim3(p->pgrid), dim3(kRealThreads), smem, ctx->stream, p->blocks,
+                                 (const PTask *)p->ptasks, (int)p->nptasks, (double *)C, (const double *)A,
+                                 (const double *)B, alpha.re, beta.re, p->part, p->pcnt, base_ok));
   } else {
-    const int grid = (int)std::min<int64_t>(p->ntiles, (int64_t)ctx->num_sms * 2);
+    if ((((uintptr_t)A | (uintptr_t)B | (uintptr_t)C) & 15) != 0)
+      return tkb_set_error(ctx, TKB_ERR_ARG, "ComplexF64 data must be 16-byte aligned");
     const size_t smem = sizeof(SmemC);
-    TKB_CUDA_TRY(ctx, cudaFuncSetAttribute(gemm_c128_kernel,
-                                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    TKB_CUDA_TRY(ctx, launch_pdl(gemm_c128_kernel, dim3(grid), dim3(256), smem, ctx->stream, p->blocks, p->tiles,
-                                 (int)p->ntiles, ctx->counters, (double2 *)C, (const double2 *)A,
-                                 (const double2 *)B, CDbl{alpha.re, alpha.im}, CDbl{beta.re, beta.im}));
+    TKB_CUDA_TRY(ctx, cudaFuncSetAttribute(gemm_c128_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    TKB_CUDA_TRY(ctx, launch_pdl(gemm_c128_kernel, dim3(p->pgrid), dim3(kCplxThreads), smem, ctx->stream, p->blocks,
+                                 (const PTask *)p->ptasks, (int)p->nptasks, (double2 *)C, (const double2 *)A,
+                                 (const double2 *)B, CDbl{alpha.re, alpha.im}, CDbl{beta.re, beta.im}, p->part,
+                                 p->pcnt));
   }
   ctx->launches++;
   TKB_CUDA_TRY(ctx, cudaGetLastError());

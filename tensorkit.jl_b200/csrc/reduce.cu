@@ -120,19 +120,15 @@ extern "C" int tkb_reduce_noalloc(int device, void *stream, int kind, int dtype,
                              std::to_string(nseg) + "); use tkb_reduce for larger tensors");
   if (nseg > 0 && (!off || !count || !stride || !weight))
     return tkb_set_error(nullptr, TKB_ERR_ARG, "null segment array");
-  // host-side staging on the stack (no heap, no device allocation)
-  RSeg segs[kNoAllocMaxSeg];
-  int64_t begin[kNoAllocMaxSeg + 1];
-  begin[0] = 0;
+  // validation (overflow-safe: count − 1 is compared with the room left after off)
+  int64_t total = 0;
   for (int64_t s = 0; s < nseg; ++s) {
     if (count[s] < 0 || off[s] < 0 || stride[s] < 0)
       return tkb_set_error(nullptr, TKB_ERR_ARG, "invalid segment");
-    if (count[s] > 0 && off[s] + (count[s] - 1) * stride[s] >= len)
+    if (count[s] > 0 && !tkb_segment_in_bounds(off[s], count[s], stride[s], len))
       return tkb_set_error(nullptr, TKB_ERR_SIZE, "segment outside the data vector");
-    segs[s] = {off[s], count[s], stride[s], weight[s]};
-    begin[s + 1] = begin[s] + count[s];
+    total += count[s];
   }
-  const int64_t total = begin[nseg];
   if (total > 0 && (!x || (kind == TKB_INNER && !y)))
     return tkb_set_error(nullptr, TKB_ERR_ARG, "null data");
 
@@ -164,10 +160,28 @@ extern "C" int tkb_reduce_noalloc(int device, void *stream, int kind, int dtype,
     host_out[0] = 0.0;
     host_out[1] = 0.0;
   } else {
-    // pageable host sources: the copies have read the stack buffers when these calls return
-    e = cudaMemcpyAsync(dsegs, segs, nseg * sizeof(RSeg), cudaMemcpyHostToDevice, st);
-    if (e == cudaSuccess)
-      e = cudaMemcpyAsync(dbegin, begin, (nseg + 1) * sizeof(int64_t), cudaMemcpyHostToDevice, st);
+    // The segment table and its prefix sums go up in chunks staged in small stack buffers
+    // (a few KiB: callers such as finalizers may run on small stacks). The sources are pageable
+    // host memory, so each copy has read its buffer when cudaMemcpyAsync returns and the buffer
+    // can be refilled.
+    constexpr int64_t kChunk = 64;
+    RSeg segs[kChunk];
+    int64_t begin[kChunk + 1];
+    int64_t run = 0;
+    for (int64_t s0 = 0; s0 < nseg && e == cudaSuccess; s0 += kChunk) {
+      const int64_t n = std::min<int64_t>(kChunk, nseg - s0);
+      for (int64_t q = 0; q < n; ++q) {
+        const int64_t s = s0 + q;
+        segs[q] = {off[s], count[s], stride[s], weight[s]};
+        begin[q] = run;
+        run += count[s];
+      }
+      begin[n] = run;
+      e = cudaMemcpyAsync(dsegs + s0, segs, n * sizeof(RSeg), cudaMemcpyHostToDevice, st);
+      // the prefix sums overlap by one entry between chunks (the same value is written twice)
+      if (e == cudaSuccess)
+        e = cudaMemcpyAsync(dbegin + s0, begin, (n + 1) * sizeof(int64_t), cudaMemcpyHostToDevice, st);
+    }
     const int nb = (int)std::max<int64_t>(1, std::min<int64_t>((total + 4095) / 4096, kNoAllocMaxCta));
     if (e == cudaSuccess) {
       if (dtype == TKB_F64)

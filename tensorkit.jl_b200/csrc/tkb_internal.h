@@ -65,6 +65,13 @@ int tkb_set_error(tkb_ctx *ctx, int code, const std::string &msg);
 
 int tkb_ensure_workspace(tkb_ctx *ctx, size_t bytes);
 
+// x[off + i·stride], i < count (count > 0, off, stride ≥ 0) lies inside [0, len): compares
+// count − 1 with the room after off instead of forming (count − 1)·stride, which could overflow
+inline bool tkb_segment_in_bounds(int64_t off, int64_t count, int64_t stride, int64_t len) {
+  if (off >= len) return false;
+  return stride == 0 || count - 1 <= (len - 1 - off) / stride;
+}
+
 // tree transform ------------------------------------------------------------------------
 struct TGroup {
   int32_t ndim;        // canonical dims (after squeezing size-1 dims and merging)
@@ -198,18 +205,21 @@ struct tkb_plan {
   int64_t expo_off = 0, expo_bytes = 0;  // exponent region inside the workspace
   void *kstiles = nullptr;      // tcgen05 product tasks (tile, K range, split slot)
   int64_t nkstiles = 0;
+  // plain precision: split-K tasks (tile, K range) in a static cost-ordered queue
+  void *ptasks = nullptr;
+  int64_t nptasks = 0;
+  int pgrid = 0;                // CTAs of the plain launch
   double *part = nullptr;       // split-K FP64 partial tiles (rewritten every launch)
-  int *pcnt = nullptr;          // split-K arrival counters (self-clearing)
-  int kcluster = 0;             // > 1: split tiles reduced inside clusters of this many CTAs
-  int slice_lk = 16;            // K values per lane in the slicing pass's warp tiles (8 or 16)
-  int kspin = 0;                // split-K pieces wait for each other (the launch is one wave)
-  void *sjobs = nullptr;        // slice jobs (block, operand)
-  int64_t *srow_begin = nullptr;
-  int nsjobs = 0;
-  int64_t nsrows = 0;
+  int *pcnt = nullptr;          // device counters (split-K arrivals; split: claims and readiness too), self-clearing
+  unsigned long long *bstat = nullptr;  // split: per-block statistics of the slicing (self-clearing)
+  int32_t *bslices = nullptr;   // split: slice count per block of the last launch, then the FP64-checked tiles
+  int slices_fixed = 0;         // split: the caller fixed the slice count
+  void *sjobs = nullptr;        // slicing tasks (block, operand, rows)
+  int64_t nsrows = 0;           // slicing tasks
   int tile_m = 64, tile_n = 64;
 };
 
+int tkb_gemm_plain_prepare(tkb_ctx *ctx, tkb_plan *p, const std::vector<GTile> &tiles);
 int tkb_gemm_launch(tkb_ctx *ctx, const tkb_plan *p, void *C, const void *A, const void *B,
                     tkb_scalar alpha, tkb_scalar beta);
 int tkb_gemm_split_prepare(tkb_ctx *ctx, tkb_plan *p);

@@ -28,7 +28,8 @@ EXPORTS = [
     "tkb_table_create",
     "tkb_table_destroy", "tkb_table_info", "tkb_treetransform", "tkb_trace_table_create",
     "tkb_trace_table_destroy", "tkb_tracetransform", "tkb_gemm_plan_create",
-    "tkb_gemm_plan_destroy", "tkb_gemm_plan_info", "tkb_grouped_gemm", "tkb_rplan_create",
+    "tkb_gemm_plan_destroy", "tkb_gemm_plan_info", "tkb_gemm_plan_slices", "tkb_grouped_gemm",
+    "tkb_rplan_create",
     "tkb_rplan_destroy", "tkb_reduce", "tkb_reduce_async", "tkb_reduce_noalloc",
     "tkb_graph_begin", "tkb_graph_end",
     "tkb_graph_launch", "tkb_graph_destroy",
@@ -102,6 +103,7 @@ def _declare(lib):
         "tkb_gemm_plan_create": ([vp, P(tkb_gemm_desc), P(vp)], C.c_int),
         "tkb_gemm_plan_destroy": ([vp], C.c_int),
         "tkb_gemm_plan_info": ([vp, P(dbl), P(i32)], C.c_int),
+        "tkb_gemm_plan_slices": ([vp, vp, vp, i64], C.c_int),
         "tkb_grouped_gemm": ([vp, vp, vp, vp, vp, tkb_scalar, tkb_scalar], C.c_int),
         "tkb_rplan_create": ([vp, i64, vp, vp, vp, vp, i64, P(vp)], C.c_int),
         "tkb_rplan_destroy": ([vp], C.c_int),

@@ -143,6 +143,16 @@ class GemmPlan:
         self.flops, self.slices = fl.value, sl.value
         self.blocks = arr
 
+    def last_slices(self):
+        """(slice count per block of the last launch, tiles the error check sent to FP64).
+        Per block: 3..7 slices, 0 = the block ran in FP64, -1 = no products (k = 0, skinny
+        block or plain precision). Waits for the library stream."""
+        nb = len(self.blocks)
+        out = np.zeros(nb + 1, dtype=np.int32)
+        L.check(self.ctx.lib.tkb_gemm_plan_slices(self.ctx.handle, self.handle, L.ptr(out), nb + 1),
+                self.ctx.handle)
+        return out[:nb].tolist(), int(out[nb])
+
     def free(self):
         if self.handle:
             self.ctx.lib.tkb_gemm_plan_destroy(self.handle)
