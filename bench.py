@@ -45,12 +45,12 @@ WORKLOADS = {
 }
 
 
-def oracle_inputs(name):
+def oracle_inputs(name, complex_=False):
     from helpers import O, cfg1_spaces, cfg2_spaces, cfg3_spaces
     if name in ("su2_large", "su2_env"):
         V, Pp = cfg2_spaces(8 if name == "su2_large" else 1)
         seed = 3 if name == "su2_large" else 1
-        return {"A": O.randn(O.Hom([V, Pp], [V]), seed), "E": O.randn(O.Hom([V], [V]), seed)}
+        return {"A": O.randn(O.Hom([V, Pp], [V]), seed, complex_), "E": O.randn(O.Hom([V], [V]), seed, complex_)}
     if name == "u1_heff":
         V, Pp, Wm = cfg3_spaces()
         Wd = Wm.flipdual()
@@ -195,6 +195,223 @@ def workload_flops(name):
     return total[0]
 
 
+def rel_errors(got, ref):
+    """Normwise max|Δ|/max|ref| and the largest elementwise |Δ|/|ref| over the entries with
+    |ref| above 1e-3·max|ref|."""
+    import numpy as np
+    got, ref = np.asarray(got), np.asarray(ref)
+    den = np.abs(ref).max()
+    big = np.abs(ref) > 1e-3 * den
+    elem = float((np.abs(got - ref)[big] / np.abs(ref)[big]).max()) if big.any() else 0.0
+    return {"normwise": float(np.abs(got - ref).max() / den), "elementwise_above_1e-3_max": elem}
+
+
+def graph_plans(expr, inputs):
+    """Captured split and plain NetworkPlans of one expression, with the launch logs of their
+    eager runs."""
+    import tensorkit_b200 as tk
+    from tensorkit_b200 import indexmanipulations as IM
+    plans, logs = {}, {}
+    for prec in ("split", "plain"):
+        p = tk.NetworkPlan(expr, precision=prec, **inputs)
+        IM.LAUNCH_LOG = []
+        p.run_eager()
+        logs[prec] = IM.LAUNCH_LOG
+        IM.LAUNCH_LOG = None
+        plans[prec] = p.capture()
+    return plans, logs
+
+
+def time_replays(plan, stream, n, warm=3):
+    """Mean device time of one of n back-to-back graph replays (CUDA events on the library stream)."""
+    import torch
+    with torch.cuda.stream(stream):
+        for _ in range(warm):
+            plan.replay()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        for _ in range(n):
+            plan.replay()
+        b.record(stream)
+        stream.synchronize()
+    return a.elapsed_time(b) / n
+
+
+def split_slices(log):
+    """Slice counts per block and FP64-checked tiles of every split grouped GEMM of a step."""
+    out = []
+    for e in log:
+        if e[0] == "gemm" and e[1].slices:
+            sl, fb = e[1].last_slices()
+            out.append({"slices": sorted(set(x for x in sl if x >= 0)), "fp64_checked_tiles": fb})
+    return out
+
+
+def other_configs(dev, ctx, flush):
+    """The other BASELINE configurations, measured in the same run as extra keys:
+    - su2_large_c128: the large SU(2) contraction in ComplexF64 (real-equivalent flops, 4 per
+      complex multiply-add), graph replays with the L2 flushed before each, split and plain;
+    - u1_heff: the U(1) two-site effective Hamiltonian as 100 back-to-back graph replays per
+      precision (its working set exceeds L2), GFLOP/s and ms/application, and its three large
+      permutes re-timed alone after the bench's write flush and after a clean flush;
+    - ad_u1su2: forward + backward (hand-written adjoint kernels) of the U(1)⊠SU(2) loss, eager,
+      ms per step."""
+    import torch
+    from helpers import to_device
+    out = {}
+    stream = ctx.stream
+
+    def flushed_ms(plan, reps=10):
+        with torch.cuda.stream(stream):
+            for _ in range(3):
+                plan.replay()
+            evs = []
+            for _ in range(reps):
+                flush.zero_()
+                a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                a.record(stream)
+                plan.replay()
+                b.record(stream)
+                evs.append((a, b))
+            stream.synchronize()
+        return statistics.mean(x.elapsed_time(y) for x, y in evs)
+
+    # ComplexF64 large SU(2)
+    tens = oracle_inputs("su2_large", complex_=True)
+    inputs = {k: to_device(v, dev) for k, v in tens.items()}
+    plans, logs = graph_plans(WORKLOADS["su2_large"]["expr"], inputs)
+    flops = sum(e[1].flops for e in logs["plain"] if e[0] == "gemm")
+    ms = {k: flushed_ms(p) for k, p in plans.items()}
+    ref = oracle_eval("su2_large", tens).data
+    out["su2_large_c128"] = {
+        "flops_per_step": flops, "unit": "GFLOP/s (real-equivalent)",
+        "split": {"value": flops / (ms["split"] * 1e-3) / 1e9, "ms_per_step": ms["split"],
+                  "max_rel_err": rel_errors(plans["split"].output.to_host(), ref),
+                  "slices": split_slices(logs["split"])},
+        "plain": {"value": flops / (ms["plain"] * 1e-3) / 1e9, "ms_per_step": ms["plain"],
+                  "max_rel_err": rel_errors(plans["plain"].output.to_host(), ref)},
+        "split_over_plain": ms["plain"] / ms["split"],
+        "l2": "flushed (256 MB write) before every replay"}
+    for p in plans.values():
+        p.free()
+
+    # U(1) two-site effective Hamiltonian, 100 replays
+    tens = oracle_inputs("u1_heff")
+    inputs = {k: to_device(v, dev) for k, v in tens.items()}
+    plans, logs = graph_plans(WORKLOADS["u1_heff"]["expr"], inputs)
+    flops = sum(e[1].flops for e in logs["plain"] if e[0] == "gemm")
+    ms = {k: time_replays(p, stream, 100) for k, p in plans.items()}
+    ref = oracle_eval("u1_heff", tens).data
+    hbm = _peaks()[0][0]
+    perms = []
+    for e in logs["split"]:
+        if e[0] != "transform":
+            continue
+        t = e[1]
+        el = e[2].data.element_size()
+        nbytes = el * (t.elems_read + t.elems_written * (1 if e[5] == 0 else 2))
+        if nbytes < (64 << 20):
+            continue
+        m_w = _retime(e, stream, flush, 10, clean=False)
+        m_c = _retime(e, stream, flush, 10, clean=True)
+        perms.append({"bytes": nbytes, "ms": m_w, "gbs": nbytes / (m_w * 1e-3) / 1e9,
+                      "frac_hbm": nbytes / (m_w * 1e-3) / 1e9 / hbm, "ms_clean_l2": m_c,
+                      "frac_hbm_clean_l2": nbytes / (m_c * 1e-3) / 1e9 / hbm})
+    out["u1_heff"] = {
+        "flops_per_application": flops, "applications": 100,
+        "split": {"gflops": flops / (ms["split"] * 1e-3) / 1e9, "ms_per_application": ms["split"],
+                  "max_rel_err": rel_errors(plans["split"].output.to_host(), ref),
+                  "slices": split_slices(logs["split"])},
+        "plain": {"gflops": flops / (ms["plain"] * 1e-3) / 1e9, "ms_per_application": ms["plain"],
+                  "max_rel_err": rel_errors(plans["plain"].output.to_host(), ref)},
+        "split_over_plain": ms["plain"] / ms["split"],
+        "large_permutes": perms,
+        "timing": "100 back-to-back graph replays (working set above L2), CUDA events"}
+    for p in plans.values():
+        p.free()
+
+    # AD step, U(1)xSU(2) (config 5)
+    import tensorkit_b200 as tk
+    from tensorkit_b200 import chainrules as CR
+    from helpers import cfg5_spaces, O
+    V, Pp = cfg5_spaces()
+    tens = {"A": O.randn(O.Hom([V, Pp], [V]), 4, True), "EL": O.randn(O.Hom([V], [V]), 41, True),
+            "ER": O.randn(O.Hom([V], [V]), 42, True)}
+    ad_in = {k: to_device(v, dev) for k, v in tens.items()}
+    expr = "f[] := EL[a;c]*A[c,p;d]*ER[d;b]*conj(A[a,p;b])"
+
+    def step():
+        o, pb = CR.network_with_pullback(expr, **ad_in)
+        return pb(tk.TensorMap(torch.ones(1, dtype=o.data.dtype, device=o.data.device), o.space))
+
+    for _ in range(3):
+        step()
+    torch.cuda.synchronize(dev)
+    times = []
+    for _ in range(10):
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize(dev)
+        a.record(stream)
+        step()
+        b.record(stream)
+        torch.cuda.synchronize(dev)
+        times.append(a.elapsed_time(b))
+    out["ad_u1su2"] = {"ms_per_step": statistics.median(times),
+                       "step": "forward + pullback of f = real(tr(E_L*A*E_R*A')) through the hand-written "
+                               "adjoint kernels, eager launches from the host, ComplexF64",
+                       "checked": "gradients vs central differences and the oracle's rule: tests/test_gpu_ad.py"}
+    return out
+
+
+def _peaks():
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+        src = "measured"
+    except Exception:
+        peaks, src = {}, "fallback"
+    return (peaks.get("hbm_gbs", 6650.0), peaks.get("bf16_tflops", 1590.0)), src
+
+
+def _retime(e, stream, flush, reps, clean):
+    """Mean device time of relaunching one logged library call after a 256 MB write flush
+    (clean: the flush buffer is read back too, so no write-back of the flush lands in the call)."""
+    import torch
+    from tensorkit_b200.indexmanipulations import relaunch
+    sink = torch.zeros(1, dtype=torch.int64, device=flush.device)
+    with torch.cuda.stream(stream):
+        for _ in range(3):
+            relaunch(e)
+        evs = []
+        for _ in range(reps):
+            flush.zero_()
+            if clean:
+                sink.copy_(flush.view(torch.int64).sum().view(1))
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            relaunch(e)
+            b.record(stream)
+            evs.append((a, b))
+        stream.synchronize()
+    return statistics.mean(x.elapsed_time(y) for x, y in evs)
+
+
+def dgemm_tflops(dev, n=4096):
+    """cuBLAS DGEMM (torch.matmul, float64) on n×n×n in this run: the FP64 tensor-core reference rate."""
+    import torch
+    a = torch.randn(n, n, dtype=torch.float64, device=dev)
+    b = torch.randn(n, n, dtype=torch.float64, device=dev)
+    for _ in range(2):
+        torch.matmul(a, b)
+    torch.cuda.synchronize(dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(5):
+        torch.matmul(a, b)
+    e1.record()
+    torch.cuda.synchronize(dev)
+    return 2.0 * n ** 3 * 5 / (e0.elapsed_time(e1) * 1e-3) / 1e12
+
+
 # ---- our arm -------------------------------------------------------------------------------
 def max_over_ranks(ms, device, world):
     """The slowest rank's time: every rank takes part in one MAX all-reduce (NCCL on GPUs,
@@ -294,9 +511,13 @@ def run_ours(args):
     out_plain = plans["plain"].output.to_host()
     err = {}
     if ref is not None:
-        den = np.abs(ref).max()
-        err = {"split": float(np.abs(out_split - ref).max() / den),
-               "plain": float(np.abs(out_plain - ref).max() / den)}
+        es, ep = rel_errors(out_split, ref), rel_errors(out_plain, ref)
+        err = {"split": es["normwise"], "plain": ep["normwise"],
+               "elementwise_above_1e-3_max": {"split": es["elementwise_above_1e-3_max"],
+                                              "plain": ep["elementwise_above_1e-3_max"]},
+               "definition": "normwise max|C - C_oracle| / max|C_oracle|; elementwise max |C - C_oracle| / "
+                             "|C_oracle| over the entries above 1e-3 max|C_oracle|",
+               "split_slices": split_slices(logs["split"])}
 
     # end to end through the public API: pinned host inputs -> device, graph, result -> host, every
     # step. Steps are pipelined the way a serving loop would run them: two captured instances of
@@ -353,8 +574,60 @@ def run_ours(args):
     ms_e2e = a.elapsed_time(b)
     ms_e2e = max_over_ranks(ms_e2e, dev, world)
 
+    # serial end to end, one step at a time (no overlap between steps): inputs up, the captured
+    # graph, the result back, then the next step. And the eager call a drop-in user makes without
+    # capture: inputs up, tk.tensor(...) (host-side lookups of the cached tables and plans, one
+    # launch per kernel), the result back.
+    P0 = plans["split"]
+
+    def serial_step():
+        with torch.cuda.stream(stream):
+            for k, v in host_in.items():
+                P0.inputs[k].data.copy_(v, non_blocking=True)
+            P0.replay()
+            host_out[0].copy_(P0.output.data, non_blocking=True)
+
+    def eager_step():
+        with torch.cuda.stream(stream), tk.using_precision("split"):
+            for k, v in host_in.items():
+                P0.inputs[k].data.copy_(v, non_blocking=True)
+            o = tk.tensor(expr, **P0.inputs)
+            host_out[1].copy_(o.data, non_blocking=True)
+
+    def host_timed(fn, n):
+        for _ in range(3):
+            fn()
+        stream.synchronize()
+        if world > 1:
+            dist.barrier()
+        ea = torch.cuda.Event(enable_timing=True)
+        eb = torch.cuda.Event(enable_timing=True)
+        ea.record(stream)
+        for _ in range(n):
+            fn()
+            stream.synchronize()  # the result is on the host before the next step starts
+        eb.record(stream)
+        stream.synchronize()
+        return max_over_ranks(ea.elapsed_time(eb), dev, world)
+
+    ms_serial = host_timed(serial_step, args.steps)
+    ms_eager = host_timed(eager_step, args.steps)
+
     # per-kernel breakdown of one split step; the dominant kernel gives the roofline entry
     roof, breakdown = kernel_roofline(args, logs["split"], ctx, flush) if rank == 0 else (None, None)
+
+    # the plain path's dominant GEMM against cuBLAS DGEMM measured in this run
+    plain_roof = None
+    if rank == 0:
+        dg = dgemm_tflops(dev)
+        _, pbd = kernel_roofline(args, logs["plain"], ctx, flush)
+        pg = max((r for r in pbd if r["kernel"] == "grouped_gemm_fp64"), key=lambda r: r["ms"])
+        plain_roof = {"kernel": "grouped_gemm_fp64 (DMMA)", "bound": "tensor", "achieved": pg["gflops"] / 1e3,
+                      "peak": dg, "unit": "TFLOP/s", "frac": pg["gflops"] / 1e3 / dg,
+                      "peak_source": "cuBLAS DGEMM 4096^3 (torch.matmul float64) measured in this run",
+                      "ms_per_launch": pg["ms"], "flops": pg["flops"]}
+    extra = other_configs(dev, ctx, flush) if (rank == 0 and world == 1 and args.workload == "su2_large"
+                                               and not args.no_extra) else None
 
     value = whole_job_value(flops, world, args.steps, ms_split)
     plain_value = whole_job_value(flops, world, args.steps, ms_plain)
@@ -369,15 +642,25 @@ def run_ours(args):
                 "config": {"workload": args.workload, "desc": WORKLOADS[args.workload]["desc"],
                            "expr": expr, "flops_per_step": flops, "l2": "flushed (256 MB write) between steps",
                            "parallelism": f"replicas x{world}", "graph": "CUDA graph per step"},
-                "plain_fp64": {"value": plain_value, "unit": "GFLOP/s", "ms_per_step": ms_plain / args.steps},
+                "plain_fp64": {"value": plain_value, "unit": "GFLOP/s", "ms_per_step": ms_plain / args.steps,
+                               "roofline": plain_roof},
                 "split_over_plain": value / plain_value,
                 "max_rel_err": err,
                 "e2e": {"value": e2e_value, "unit": "GFLOP/s", "h2d_bytes_per_step": h2d,
                         "d2h_bytes_per_step": d2h, "ms_per_step": ms_e2e / args.steps,
                         "pipelined": "inputs of step i+1 up and result of step i-1 back on copy streams "
                                      "while step i computes (two captured instances)"},
+                "e2e_serial": {"value": whole_job_value(flops, world, args.steps, ms_serial), "unit": "GFLOP/s",
+                               "ms_per_step": ms_serial / args.steps,
+                               "step": "inputs up, graph replay, result back, host waits; no overlap between steps"},
+                "e2e_eager": {"value": whole_job_value(flops, world, args.steps, ms_eager), "unit": "GFLOP/s",
+                              "ms_per_step": ms_eager / args.steps,
+                              "step": "inputs up, tk.tensor(expr) without capture (eager launches), result back, "
+                                      "host waits"},
                 "gpu_launches": (plans["split"].kernels_per_replay) * args.steps,
                 "roofline": roof, "breakdown": breakdown, "cpu_baseline": cpu, "clocks": clocks}
+        if extra is not None:
+            line["configs"] = extra
         print(json.dumps(line))
     for p in list(plans.values()) + [twin]:
         p.free()
@@ -451,8 +734,18 @@ def kernel_roofline(args, log, ctx, flush):
             else:
                 plan = e[1]
                 S = plan.slices
-                rows.append({"kernel": "grouped_gemm_split" if S else "grouped_gemm_fp64", "ms": ms,
-                             "flops": plan.flops, "gflops": plan.flops / (ms * 1e-3) / 1e9, "slices": S})
+                row = {"kernel": "grouped_gemm_split" if S else "grouped_gemm_fp64", "ms": ms,
+                       "flops": plan.flops, "gflops": plan.flops / (ms * 1e-3) / 1e9, "slices": S}
+                if S:
+                    # int8 work of the launch: S_b(S_b + 1)/2 products of 2mnk per block at the
+                    # slice count each block used (blocks in FP64 count their FP64 flops apart)
+                    sl, fb = plan.last_slices()
+                    mul = 4 if plan.is_complex else 1
+                    ops8 = sum(2.0 * m * n * k * mul * sb * (sb + 1) / 2
+                               for (m, n, k), sb in zip(plan.blocks[:, :3].tolist(), sl) if sb > 0)
+                    row.update({"int8_ops": ops8, "block_slices": sorted(set(x for x in sl if x >= 0)),
+                                "fp64_checked_tiles": fb})
+                rows.append(row)
     dom = max(rows, key=lambda r: r["ms"])
     total = sum(r["ms"] for r in rows)
     for r in rows:
@@ -464,19 +757,33 @@ def kernel_roofline(args, log, ctx, flush):
     else:
         S = dom.get("slices") or 0
         if S:
-            ops = dom["flops"] * S * (S + 1) / 2
+            ops = dom["int8_ops"]
             ach = ops / (dom["ms"] * 1e-3) / 1e12
             peak = 2.0 * bf16
-            roof = {"kernel": "grouped_gemm_split (slice pass + int8 tensor-core products)",
+            roof = {"kernel": "gemm_split_fused_kernel (slicing + int8 tensor-core products + FP64 "
+                              "recombination, one launch)",
                     "bound": "tensor", "achieved": ach, "peak": peak, "unit": "TFLOP/s",
-                    "frac": ach / peak, "traffic": None,
+                    "frac": ach / peak, "traffic": profile_traffic("gemm_split_fused_su2_large"),
                     "peak_source": f"2 x bf16_tflops of {src} peaks (int8 dense = 2 x bf16 dense)",
-                    "algorithmic": f"S(S+1)/2 = {S * (S + 1) // 2} int8 products of 2mnk = {dom['flops']:.4e}",
+                    "algorithmic": f"sum over blocks of S_b(S_b+1)/2 int8 products of 2mnk = {ops:.4e} "
+                                   f"(slice counts {dom['block_slices']})",
                     "fp64_equiv_gflops": dom["gflops"], "ms_per_launch": dom["ms"]}
         else:
             roof = {"kernel": "grouped_gemm_fp64", "bound": "tensor", "achieved": dom["gflops"] / 1e3,
                     "peak": None, "unit": "TFLOP/s", "frac": None, "traffic": None}
     return roof, rows
+
+
+def profile_traffic(name):
+    """DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum) of a kernel from its
+    committed ncu summary profiles/<name>.md (a line `traffic_bytes_per_launch: N`), else None."""
+    try:
+        for ln in open(os.path.join(ROOT, "profiles", name + ".md")):
+            if ln.strip().startswith("traffic_bytes_per_launch:"):
+                return float(ln.split(":", 1)[1].split()[0])
+    except (OSError, ValueError, IndexError):
+        pass
+    return None
 
 
 def cpu_baseline(args, tens_o, flops):
@@ -507,6 +814,8 @@ def main():
                     help="time one block factorization of the workload's first input instead")
     ap.add_argument("--precision", default="split", choices=["split", "plain"])
     ap.add_argument("--reps", type=int, default=3)
+    ap.add_argument("--no-extra", action="store_true",
+                    help="skip the other configurations (ComplexF64, U(1) effective Hamiltonian, AD step)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

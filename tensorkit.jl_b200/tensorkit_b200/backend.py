@@ -142,6 +142,7 @@ class GemmPlan:
         L.check(ctx.lib.tkb_gemm_plan_info(h, C.byref(fl), C.byref(sl)))
         self.flops, self.slices = fl.value, sl.value
         self.blocks = arr
+        self.is_complex = dtype_code == L.TKB_C128
 
     def last_slices(self):
         """(slice count per block of the last launch, tiles the error check sent to FP64).
