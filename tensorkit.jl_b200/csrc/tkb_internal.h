@@ -98,6 +98,9 @@ struct TaskRec {
   int32_t ta, tb;            // tile extents (powers of two; row tiles: ta = na, tb = nb)
   int32_t mode;              // 0: same fastest dim on both sides, 1: transpose
   uint32_t mul;              // row tiles: ⌊(2³²−1)/na⌋ + 1, so e / na = umulhi(e, mul) for e < 2¹⁶
+  uint32_t mul2 = 0;         // row tiles copied in pairs: the same for na / 2
+  int32_t pairs = 0;         // row tiles: 1 when the rows are contiguous on both sides and every
+                             // row starts at an even element, so 16-byte pairs stay aligned
 };
 
 struct tkb_table {
@@ -122,6 +125,7 @@ struct tkb_table {
   // (na = the fast extent, not rounded to a power of two) for the register row-copy kernel
   int64_t nrow_tasks = 0;
   TaskRec *row_rec = nullptr;
+  int64_t row_pair_elems = 0;     // elements of row tasks that 16-byte pair accesses can copy
 };
 
 int tkb_transform_launch(tkb_ctx *ctx, const tkb_table *t, int dtype, void *dst,

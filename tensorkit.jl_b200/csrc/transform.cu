@@ -30,6 +30,7 @@ namespace {
 
 constexpr int kThreads = 256;
 constexpr int kBatch = 8;  // elements per thread per load batch (loads in flight per thread)
+constexpr int kBatchPairs = kBatch / 2;  // 16-byte pairs per thread per batch
 constexpr int64_t kTileElemsMax = 2048;  // largest task (= kThreads * kBatch elements)
 constexpr size_t kSmemBudget = 96 * 1024;
 constexpr int kTaskWords = 2 + TKB_MAX_IND;  // per task: tile a, tile b, outer multi-index
@@ -350,10 +351,10 @@ __global__ void __launch_bounds__(kThreads)
 // by the precomputed reciprocal `mul` (exact for tile indices below 2¹⁶: Granlund–Montgomery
 // division by invariant integers). Without shared-memory tiles the kernel runs at the
 // occupancy its registers allow, which keeps enough loads in flight per SM for HBM.
-template <typename T, bool CONJ, typename OFF>
-__global__ void __launch_bounds__(kThreads, sizeof(T) == 8 ? 6 : 4)
+template <typename T, bool CONJ, typename OFF, bool PAIRS>
+__global__ void __launch_bounds__(kThreads, (sizeof(T) == 8 && !PAIRS) ? 6 : 4)
     treetransform_rows_kernel(const TaskRec *__restrict__ recs, int64_t ntasks, T *__restrict__ dst,
-                              const T *__restrict__ src, CDbl alpha_, CDbl beta_, int beta_zero) {
+                              const T *__restrict__ src, CDbl alpha_, CDbl beta_, int beta_zero, int pairs_ok) {
   __shared__ TaskRec rs[kRecCache];
   const T alpha = scalar_from<T>(alpha_);
   const T beta = scalar_from<T>(beta_);
@@ -373,6 +374,44 @@ __global__ void __launch_bounds__(kThreads, sizeof(T) == 8 ? 6 : 4)
 
   for (int64_t task = t_begin; task < t_end; ++task) {
     const TaskRec &R = rs[task - t_begin];
+    if constexpr (PAIRS) {
+      if (R.pairs && pairs_ok) {
+        // real rows contiguous on both sides: 16-byte loads and stores of element pairs (half as
+        // many per thread and batch: the same bytes in flight)
+        const int np = R.na / 2, nun = np * R.nb;
+        const uint32_t mul2 = R.mul2;
+        const double u = R.u;
+        const double2 *sb2 = reinterpret_cast<const double2 *>(src + R.sbase);
+        double2 *db2 = reinterpret_cast<double2 *>(dst + R.dbase);
+        const OFF sB2 = (OFF)(R.sB / 2), dB2 = (OFF)(R.dB / 2);
+        const double a = scalar_from<double>(alpha_), bb = scalar_from<double>(beta_);
+        for (int e0 = 0; e0 < nun; e0 += kThreads * kBatchPairs) {
+          double2 v[kBatchPairs];
+#pragma unroll
+          for (int q = 0; q < kBatchPairs; ++q) {
+            const int e = e0 + q * kThreads + threadIdx.x;
+            const int row = mul2 ? (int)__umulhi((unsigned)e, mul2) : e, cp = e - row * np;
+            if (e < nun) v[q] = __ldg(sb2 + (OFF)cp + (OFF)row * sB2);
+          }
+#pragma unroll
+          for (int q = 0; q < kBatchPairs; ++q) {
+            const int e = e0 + q * kThreads + threadIdx.x;
+            const int row = mul2 ? (int)__umulhi((unsigned)e, mul2) : e, cp = e - row * np;
+            if (e < nun) {
+              double2 *dp = db2 + (OFF)cp + (OFF)row * dB2;
+              double2 r = make_double2(a * (u * v[q].x), a * (u * v[q].y));
+              if (!bz) {
+                const double2 o = *dp;
+                r.x = fma(bb, o.x, r.x);
+                r.y = fma(bb, o.y, r.y);
+              }
+              *dp = r;
+            }
+          }
+        }
+        continue;
+      }
+    }
     const int na = R.na, nel = R.na * R.nb;
     const uint32_t mul = R.mul;
     const OFF sA = (OFF)R.sA, sB = (OFF)R.sB, dA = (OFF)R.dA, dB = (OFF)R.dB;
@@ -463,6 +502,7 @@ extern "C" int tkb_table_create(tkb_ctx *ctx, const tkb_table_desc *d, tkb_table
   std::vector<TaskRec> hrec;   // task → tree-0 bases and extents (single-tree tables)
   std::vector<TaskRec> hrow;   // exact row tiles (single-tree tables, every group mode 0)
   bool all_off32 = true, all_rows = true, row_off32 = true;
+  int64_t row_pair_elems = 0;  // elements of row tasks that can be copied in 16-byte pairs
   int64_t row_transposed = 0;  // elements of transpose groups in the row tiles
   std::vector<double> hcoef;
   int64_t ntasks = 0, er = 0, ew = 0;
@@ -731,6 +771,13 @@ extern "C" int tkb_table_create(tkb_ctx *ctx, const tkb_table_desc *d, tkb_table
             rec.tb = rec.nb;
             rec.mode = 0;
             rec.mul = rec.na > 1 ? 0xFFFFFFFFu / (uint32_t)rec.na + 1u : 0u;
+            // 16-byte pairs: contiguous rows on both sides, even row length and even row starts
+            rec.pairs = (tg.mode == 0 && rec.sA == 1 && rec.dA == 1 && rec.na % 2 == 0 && rec.sbase % 2 == 0 &&
+                         rec.dbase % 2 == 0 && (rec.nb == 1 || (rec.sB % 2 == 0 && rec.dB % 2 == 0)))
+                            ? 1
+                            : 0;
+            rec.mul2 = rec.na > 2 ? 0xFFFFFFFFu / (uint32_t)(rec.na / 2) + 1u : 0u;
+            if (rec.pairs) row_pair_elems += (int64_t)rec.na * rec.nb;
             hrow.push_back(rec);
           }
         }
@@ -755,6 +802,7 @@ extern "C" int tkb_table_create(tkb_ctx *ctx, const tkb_table_desc *d, tkb_table
   // the row kernel takes the table when its transpose groups are a small remainder (sub-blocks
   // whose leading leg has dimension 1, for example); otherwise the staged ring transposes
   if (t->single_tree && all_rows && row_off32 && row_transposed * 64 <= er) t->nrow_tasks = (int64_t)hrow.size();
+  t->row_pair_elems = row_pair_elems;
   t->smem_f64 = smem_max_f64;
   t->smem_c128 = smem_max_c128;
   t->src_len = d->src_len;
@@ -821,16 +869,22 @@ int tkb_transform_launch(tkb_ctx *ctx, const tkb_table *t, int dtype, void *dst,
     if (dtype == TKB_F64 && (alpha.im != 0.0 || beta.im != 0.0))
       return tkb_set_error(ctx, TKB_ERR_ARG, "complex scalar with real data");
     // persistent CTAs: as many as reside at once, with at most kRecCache tasks each
-    using KD = void (*)(const TaskRec *, int64_t, double *, const double *, CDbl, CDbl, int);
-    using KC = void (*)(const TaskRec *, int64_t, double2 *, const double2 *, CDbl, CDbl, int);
+    using KD = void (*)(const TaskRec *, int64_t, double *, const double *, CDbl, CDbl, int, int);
+    using KC = void (*)(const TaskRec *, int64_t, double2 *, const double2 *, CDbl, CDbl, int, int);
     KD kd = nullptr;
     KC kc = nullptr;
     const void *kfn;
+    // 16-byte pair accesses need 16-byte aligned data vectors
+    const int pairs_ok = ((((uintptr_t)dst | (uintptr_t)src) & 15) == 0) ? 1 : 0;
     if (dtype == TKB_F64) {
-      kd = treetransform_rows_kernel<double, false, int32_t>;
+      // the kernel with the 16-byte pair path (fewer resident CTAs) when most of the table can
+      // use it, else the scalar one
+      kd = (pairs_ok && t->row_pair_elems * 2 >= t->elems_read) ? treetransform_rows_kernel<double, false, int32_t, true>
+                                                                : treetransform_rows_kernel<double, false, int32_t, false>;
       kfn = (const void *)kd;
     } else {
-      kc = conj ? treetransform_rows_kernel<double2, true, int32_t> : treetransform_rows_kernel<double2, false, int32_t>;
+      kc = conj ? treetransform_rows_kernel<double2, true, int32_t, false>
+                : treetransform_rows_kernel<double2, false, int32_t, false>;
       kfn = (const void *)kc;
     }
     const int per_sm = tkb_occupancy(ctx->device, kfn, kThreads, 0);
@@ -840,10 +894,10 @@ int tkb_transform_launch(tkb_ctx *ctx, const tkb_table *t, int dtype, void *dst,
     pg = std::max<int64_t>(pg, (nt + kRecCache - 1) / kRecCache);
     if (kd)
       TKB_CUDA_TRY(ctx, launch_pdl(kd, dim3((int)pg), dim3(kThreads), 0, ctx->stream, t->row_rec, nt,
-                                   (double *)dst, (const double *)src, a, b, bz));
+                                   (double *)dst, (const double *)src, a, b, bz, pairs_ok));
     else
       TKB_CUDA_TRY(ctx, launch_pdl(kc, dim3((int)pg), dim3(kThreads), 0, ctx->stream, t->row_rec, nt,
-                                   (double2 *)dst, (const double2 *)src, a, b, bz));
+                                   (double2 *)dst, (const double2 *)src, a, b, bz, pairs_ok));
     ctx->launches++;
     TKB_CUDA_TRY(ctx, cudaGetLastError());
     return TKB_OK;
