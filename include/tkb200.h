@@ -162,6 +162,16 @@ typedef struct tkb_gemm_desc {
 } tkb_gemm_desc;
 
 int tkb_gemm_plan_create(tkb_ctx *ctx, const tkb_gemm_desc *desc, tkb_plan **out);
+/* The same plan with the work-decomposition knobs set by the caller (an autotuner): when the
+ * output tiles alone would leave SMs idle, the K loops are cut into at most max_pieces pieces
+ * (1..64; 1 = no split K) of at least min_piece_steps K steps (BK = 16 plain, 32 split).
+ * tkb_gemm_plan_create uses max_pieces = 8, min_piece_steps = 4. (No reference counterpart.) */
+typedef struct tkb_gemm_tuning {
+  int32_t max_pieces;
+  int32_t min_piece_steps;
+} tkb_gemm_tuning;
+int tkb_gemm_plan_create_tuned(tkb_ctx *ctx, const tkb_gemm_desc *desc, const tkb_gemm_tuning *tuning,
+                               tkb_plan **out);
 int tkb_gemm_plan_destroy(tkb_plan *plan);
 /* flops (real, 2mnk per real block, 8mnk per complex block) and the slice count used */
 int tkb_gemm_plan_info(const tkb_plan *plan, double *flops, int32_t *slices);

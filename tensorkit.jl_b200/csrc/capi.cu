@@ -38,7 +38,7 @@ int tkb_ensure_workspace(tkb_ctx *ctx, size_t bytes) {
 
 extern "C" {
 
-int tkb_version(void) { return 100; }
+int tkb_version(void) { return 200; }
 
 const char *tkb_last_error(const tkb_ctx *ctx) {
   if (ctx) return ctx->err.c_str();
@@ -173,7 +173,20 @@ static bool in_bounds(int64_t off, int64_t rows, int64_t cols, int64_t ld, int64
   return off + (rows - 1) + (cols - 1) * ld < len;
 }
 
+static int plan_create(tkb_ctx *ctx, const tkb_gemm_desc *d, const tkb_gemm_tuning *tn, tkb_plan **out);
+
 int tkb_gemm_plan_create(tkb_ctx *ctx, const tkb_gemm_desc *d, tkb_plan **out) {
+  return plan_create(ctx, d, nullptr, out);
+}
+
+int tkb_gemm_plan_create_tuned(tkb_ctx *ctx, const tkb_gemm_desc *d, const tkb_gemm_tuning *t, tkb_plan **out) {
+  if (!t) return tkb_set_error(ctx, TKB_ERR_ARG, "null tuning");
+  if (t->max_pieces < 1 || t->max_pieces > 64 || t->min_piece_steps < 1)
+    return tkb_set_error(ctx, TKB_ERR_ARG, "tuning: max_pieces must be in 1..64, min_piece_steps at least 1");
+  return plan_create(ctx, d, t, out);
+}
+
+static int plan_create(tkb_ctx *ctx, const tkb_gemm_desc *d, const tkb_gemm_tuning *tn, tkb_plan **out) {
   if (!ctx || !d || !out) return tkb_set_error(ctx, TKB_ERR_ARG, "null argument");
   *out = nullptr;
   if (d->dtype != TKB_F64 && d->dtype != TKB_C128) return tkb_set_error(ctx, TKB_ERR_ARG, "unknown dtype");
@@ -190,6 +203,10 @@ int tkb_gemm_plan_create(tkb_ctx *ctx, const tkb_gemm_desc *d, tkb_plan **out) {
   p->precision = d->precision;
   p->slices = d->slices;
   p->nblocks = nb;
+  if (tn) {
+    p->max_pieces = tn->max_pieces;
+    p->min_piece_steps = tn->min_piece_steps;
+  }
   p->lenA = d->lenA;
   p->lenB = d->lenB;
   p->lenC = d->lenC;

@@ -581,11 +581,6 @@ int tkb_gemm_skinny_launch(tkb_ctx *ctx, const tkb_plan *p, void *C, const void 
   return TKB_OK;
 }
 
-namespace {
-constexpr int kMinPieceSteps = 4;  // K steps of BK per split-K piece, at least
-constexpr int kMaxPieces = 8;      // pieces per tile, at most
-}  // namespace
-
 int tkb_gemm_plain_prepare(tkb_ctx *ctx, tkb_plan *p, const std::vector<GTile> &tiles) {
   const bool cplx = p->dtype == TKB_C128;
   const void *kfn = cplx ? (const void *)gemm_c128_kernel : (const void *)gemm_f64_kernel;
@@ -604,12 +599,12 @@ int tkb_gemm_plain_prepare(tkb_ctx *ctx, tkb_plan *p, const std::vector<GTile> &
     maxnk = std::max(maxnk, nks[i]);
   }
   auto pieces = [&](int64_t nk, int64_t target) {
-    return (int)std::min<int64_t>(kMaxPieces, std::max<int64_t>(1, (nk + target - 1) / target));
+    return (int)std::min<int64_t>(p->max_pieces, std::max<int64_t>(1, (nk + target - 1) / target));
   };
-  // the shortest piece length (at least kMinPieceSteps) whose tasks still fit the resident slots
+  // the shortest piece length (at least min_piece_steps) whose tasks still fit the resident slots
   int64_t target = maxnk;
   if (nt < slots) {
-    target = std::max<int64_t>(kMinPieceSteps, (total + slots - 1) / slots);
+    target = std::max<int64_t>(p->min_piece_steps, (total + slots - 1) / slots);
     for (; target < maxnk; ++target) {
       int64_t cnt = 0;
       for (int64_t i = 0; i < nt; ++i) cnt += pieces(nks[i], target);

@@ -1363,7 +1363,7 @@ int tkb_gemm_split_prepare(tkb_ctx *ctx, tkb_plan *p) {
     return p->hblocks[x.block].kpad > p->hblocks[y.block].kpad;
   });
   // products items of the persistent kernel (one CTA per SM). With fewer tiles than SMs the K
-  // loops are cut into pieces of about `target` stages, the smallest target (≥ 4 stages) whose
+  // loops are cut into pieces of about `target` stages, the smallest target (≥ min_piece_steps) whose
   // item count still fits one round of the CTAs, so the longest item is as short as possible.
   std::vector<SplitTile> kt;
   int nslots = 0, npart = 0;
@@ -1379,11 +1379,12 @@ int tkb_gemm_split_prepare(tkb_ctx *ctx, tkb_plan *p) {
     // int32 accumulators stay exact over at most (2^31 − 1)/(S·127²) K positions per item
     const int64_t maxst = std::max<int64_t>(1, (int64_t)2147483647 / ((int64_t)S * 127 * 127) / KSTAGE);
     auto pieces = [&](int64_t nk, int64_t target) {
-      return (int)std::max<int64_t>(std::min<int64_t>(8, (nk + target - 1) / target), (nk + maxst - 1) / maxst);
+      return (int)std::max<int64_t>(std::min<int64_t>(p->max_pieces, (nk + target - 1) / target),
+                                    (nk + maxst - 1) / maxst);
     };
     int64_t target = maxnk;  // no split
     if (nt < nsm) {
-      target = std::max<int64_t>(4, (total + nsm - 1) / nsm);
+      target = std::max<int64_t>(p->min_piece_steps, (total + nsm - 1) / nsm);
       for (; target < maxnk; ++target) {
         int64_t cnt = 0;
         for (const GTile &t : tiles) cnt += t.kind == 0 ? pieces(p->hblocks[t.block].kpad / KSTAGE, target) : 1;

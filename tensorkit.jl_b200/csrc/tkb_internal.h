@@ -221,6 +221,8 @@ struct tkb_plan {
   void *sjobs = nullptr;        // slicing tasks (block, operand, rows)
   int64_t nsrows = 0;           // slicing tasks
   int tile_m = 64, tile_n = 64;
+  // split-K knobs (tkb_gemm_plan_create_tuned): pieces per tile at most, K steps per piece at least
+  int max_pieces = 8, min_piece_steps = 4;
 };
 
 int tkb_gemm_plain_prepare(tkb_ctx *ctx, tkb_plan *p, const std::vector<GTile> &tiles);

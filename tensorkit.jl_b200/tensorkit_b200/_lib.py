@@ -27,7 +27,7 @@ EXPORTS = [
     "tkb_ctx_synchronize", "tkb_selftest_bounded_wait", "tkb_ctx_launch_count", "tkb_last_error",
     "tkb_table_create",
     "tkb_table_destroy", "tkb_table_info", "tkb_treetransform", "tkb_trace_table_create",
-    "tkb_trace_table_destroy", "tkb_tracetransform", "tkb_gemm_plan_create",
+    "tkb_trace_table_destroy", "tkb_tracetransform", "tkb_gemm_plan_create", "tkb_gemm_plan_create_tuned",
     "tkb_gemm_plan_destroy", "tkb_gemm_plan_info", "tkb_gemm_plan_slices", "tkb_grouped_gemm",
     "tkb_rplan_create",
     "tkb_rplan_destroy", "tkb_reduce", "tkb_reduce_async", "tkb_reduce_noalloc",
@@ -71,6 +71,10 @@ class tkb_gemm_desc(C.Structure):
     ]
 
 
+class tkb_gemm_tuning(C.Structure):
+    _fields_ = [("max_pieces", C.c_int32), ("min_piece_steps", C.c_int32)]
+
+
 class TKBError(RuntimeError):
     def __init__(self, code, msg):
         super().__init__(f"libtkb200 error {code}: {msg}")
@@ -101,6 +105,7 @@ def _declare(lib):
         "tkb_trace_table_destroy": ([vp], C.c_int),
         "tkb_tracetransform": ([vp, vp, C.c_int, vp, vp, tkb_scalar, tkb_scalar, C.c_int], C.c_int),
         "tkb_gemm_plan_create": ([vp, P(tkb_gemm_desc), P(vp)], C.c_int),
+        "tkb_gemm_plan_create_tuned": ([vp, P(tkb_gemm_desc), P(tkb_gemm_tuning), P(vp)], C.c_int),
         "tkb_gemm_plan_destroy": ([vp], C.c_int),
         "tkb_gemm_plan_info": ([vp, P(dbl), P(i32)], C.c_int),
         "tkb_gemm_plan_slices": ([vp, vp, vp, i64], C.c_int),

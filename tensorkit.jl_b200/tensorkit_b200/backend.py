@@ -119,8 +119,9 @@ class DeviceTable:
 
 
 class GemmPlan:
-    def __init__(self, ctx: "Context", blocks, lens, dtype_code, precision_code, slices):
-        """blocks: list of (m, n, k, offA, offB, offC, lda, ldb, ldc, opA, opB)."""
+    def __init__(self, ctx: "Context", blocks, lens, dtype_code, precision_code, slices, tuning=None):
+        """blocks: list of (m, n, k, offA, offB, offC, lda, ldb, ldc, opA, opB); tuning:
+        (max_pieces, min_piece_steps) of the split-K decomposition, or None for the default."""
         self.ctx = ctx
         nb = len(blocks)
         arr = np.array(blocks, dtype=np.int64).reshape(nb, 11) if nb else np.zeros((0, 11), np.int64)
@@ -136,8 +137,14 @@ class GemmPlan:
         d.precision = precision_code
         d.slices = slices
         h = C.c_void_p()
-        L.check(ctx.lib.tkb_gemm_plan_create(ctx.handle, C.byref(d), C.byref(h)), ctx.handle)
+        if tuning is None:
+            L.check(ctx.lib.tkb_gemm_plan_create(ctx.handle, C.byref(d), C.byref(h)), ctx.handle)
+        else:
+            tn = L.tkb_gemm_tuning(int(tuning[0]), int(tuning[1]))
+            L.check(ctx.lib.tkb_gemm_plan_create_tuned(ctx.handle, C.byref(d), C.byref(tn), C.byref(h)),
+                    ctx.handle)
         self.handle = h
+        self.tuning = tuning
         fl, sl = C.c_double(), C.c_int32()
         L.check(ctx.lib.tkb_gemm_plan_info(h, C.byref(fl), C.byref(sl)))
         self.flops, self.slices = fl.value, sl.value

@@ -84,38 +84,64 @@ def gemm_plan(ctx, tC, tA, tB, prec=None, slices=None):
     return ctx.plans.get_or(key, make)
 
 
-def _autotune(ctx, tC, tA, tB, blocks, lens, code, sl, reps=5):
-    """Precision "auto": build the plain FP64 and the split-precision plan of this block
-    structure, time both on the operands at hand (into a scratch output, CUDA events on the
-    library stream) and keep the faster; the choice is cached with the plan, per
-    (structure, dtype). Both forms meet the 1e-12 relative bound on the workloads."""
+def _autotune(ctx, tC, tA, tB, blocks, lens, code, sl, reps=5, cache=None):
+    """Precision "auto": the tuner of `tuning.py` over precision (plain FP64 / split) and the
+    split-K decomposition, per (block structure, dtype, device). A structure already in the
+    on-disk cache gets its recorded choice without any timing; otherwise every candidate runs on
+    the operands at hand into a scratch output (CUDA events on the library stream), candidates
+    whose result differs from the plain FP64 result by more than 1e-12 (normwise) are rejected,
+    the fastest is kept and recorded."""
     import torch
-    cands = {m: GemmPlan(ctx, blocks, lens, code, L.TKB_SPLIT_INT8 if m == "split" else L.TKB_PLAIN, sl)
-             for m in ("plain", "split")}
+    from . import tuning as T
+    cache = cache if cache is not None else T.default_cache()
+    key = T.structure_key(blocks, code, torch.cuda.get_device_name(ctx.device), L.load().tkb_version())
+
+    def build(c):
+        mode, maxp, minst = c
+        return GemmPlan(ctx, blocks, lens, code, L.TKB_SPLIT_INT8 if mode == "split" else L.TKB_PLAIN, sl,
+                        tuning=(maxp, minst))
+
+    rec = cache.get(key)
+    if rec is not None:
+        plan = build(tuple(rec["choice"]))
+        plan.tuned = dict(rec, cached=True)
+        return plan
     scratch = torch.empty_like(tC.data)
-    times = {}
+    ref = None
     _sync_in(ctx)
-    with torch.cuda.stream(ctx.stream):
-        for m, plan in cands.items():
+
+    def measure(c):
+        nonlocal ref
+        plan = build(c)
+        try:
             def go():
                 L.check(ctx.lib.tkb_grouped_gemm(ctx.handle, plan.handle, C.c_void_p(scratch.data_ptr()),
                                                  C.c_void_p(tA.data.data_ptr()), C.c_void_p(tB.data.data_ptr()),
                                                  _scalar(1.0), _scalar(0.0)), ctx.handle)
-            for _ in range(2):
-                go()
-            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            a.record(ctx.stream)
-            for _ in range(reps):
-                go()
-            b.record(ctx.stream)
-            ctx.stream.synchronize()
-            times[m] = a.elapsed_time(b) / reps * 1e3
-    best = min(times, key=times.get)
-    for m, plan in cands.items():
-        if m != best:
+            with torch.cuda.stream(ctx.stream):
+                for _ in range(2):
+                    go()
+                a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                a.record(ctx.stream)
+                for _ in range(reps):
+                    go()
+                b.record(ctx.stream)
+                ctx.stream.synchronize()
+            us = a.elapsed_time(b) / reps * 1e3
+            if ref is None:  # the first candidate is plain FP64: the reference result
+                ref = scratch.clone()
+                return us, None
+            den = ref.abs().max().item()
+            err = (scratch - ref).abs().max().item() / den if den > 0 else 0.0
+            return us, err
+        finally:
             plan.free()
-    cands[best].tuned = {"choice": best, "us": times}
-    return cands[best]
+
+    best, rec = T.select(T.CANDIDATES, measure)
+    cache.put(key, rec)
+    plan = build(best)
+    plan.tuned = dict(rec, cached=False)
+    return plan
 
 
 def mul_(tC: TensorMap, tA, tB, alpha=1.0, beta=0.0, prec=None, slices=None):
