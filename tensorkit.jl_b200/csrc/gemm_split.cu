@@ -302,6 +302,37 @@ __device__ __forceinline__ void store_piece(const typename SrcVal<CPLX>::T (&v)[
 // row", and the largest row 2-norms as double bits)
 constexpr int kExpBias = 4096;
 
+// Per-row maximum and sum of squares of the lanes of a warp (all lanes call; row −1 = no value).
+// The lanes holding one row form runs of consecutive lanes (a row can recur later in the warp);
+// every run is reduced to its first lane with a windowed shuffle reduction keyed by the run's
+// first lane, and that lane adds the run's values with one shared-memory atomic each.
+__device__ __forceinline__ void warp_row_account(int row, double m, double s2, unsigned long long *rmax, double *rsq) {
+  const unsigned full = 0xffffffffu;
+  const int lane = threadIdx.x & 31;
+  const int rp = __shfl_up_sync(full, row, 1);
+  const bool head = lane == 0 || rp != row;
+  int start = head ? lane : 0;  // first lane of this lane's run: a prefix maximum of the heads
+#pragma unroll
+  for (int d = 1; d < 32; d <<= 1) {
+    const int o = __shfl_up_sync(full, start, d);
+    if (lane >= d) start = max(start, o);
+  }
+#pragma unroll
+  for (int d = 1; d < 32; d <<= 1) {
+    const int so = __shfl_down_sync(full, start, d);
+    const double mo = __shfl_down_sync(full, m, d);
+    const double qo = __shfl_down_sync(full, s2, d);
+    if (lane + d < 32 && so == start) {
+      m = fmax(m, mo);
+      s2 += qo;
+    }
+  }
+  if (head && row >= 0 && m > 0.0) {
+    atomicMax(&rmax[row], (unsigned long long)__double_as_longlong(m));
+    atomicAdd(&rsq[row], s2);
+  }
+}
+
 // One slicing task with the NT threads of the CTA. rmax, rsq (zeroed by the caller) and rexp
 // are per-row shared-memory scratch of kSliceMaxRows entries; bst receives the block statistics.
 template <int S, bool CPLX, bool ROWC, int NT>
@@ -344,37 +375,44 @@ __device__ __forceinline__ void slice_task(const GBlock &b, const SliceTask &tas
     const int64_t r = task.r0 + row;
     load_piece<CPLX, ROWC, LK>(X, xo + r * rs, ks, c, b.k, r < msrc, v);
   };
-  auto account = [&](const T (&v)[LK], int row) {
+  // a piece's maximum magnitude and sum of squares, combined per row: first over the runs of
+  // lanes of the warp that hold the same row (every lane takes part; lanes without a piece pass
+  // row −1), then one shared-memory atomic per run
+  auto account = [&](const T (&v)[LK], int row, bool active) {
     double m = 0.0, s2 = 0.0;
+    if (active) {
 #pragma unroll
-    for (int l = 0; l < LK; ++l) {
-      m = fmax(m, absmax(v[l]));
-      s2 += sq_of(v[l]);
+      for (int l = 0; l < LK; ++l) {
+        m = fmax(m, absmax(v[l]));
+        s2 += sq_of(v[l]);
+      }
+    } else {
+      row = -1;
     }
-    if (m > 0.0) {
-      atomicMax(&rmax[row], (unsigned long long)__double_as_longlong(m));
-      atomicAdd(&rsq[row], s2);
-    }
+    warp_row_account(row, m, s2, rmax, rsq);
   };
 
   // phase 1: row maxima and sums of squares; the first kSliceKeep pieces stay in registers
+  // (the loops run warp-uniformly: every lane of a warp reaches the warp reductions together)
+  const int wbase = tid & ~31, lane = tid & 31;
   T keep[kSliceKeep][LK];
 #pragma unroll
   for (int q = 0; q < kSliceKeep; ++q) {
     const int p = tid + q * NT;
-    if (p < npieces) {
-      int row;
-      int64_t c;
-      load(p, keep[q], row, c);
-      account(keep[q], row);
-    }
+    int row = 0;
+    int64_t c = 0;
+    const bool act = p < npieces;
+    if (act) load(p, keep[q], row, c);
+    account(keep[q], row, act);
   }
-  for (int p = tid + kSliceKeep * NT; p < npieces; p += NT) {
+  for (int p0 = wbase + kSliceKeep * NT; p0 < npieces; p0 += NT) {
+    const int p = p0 + lane;
     T v[LK];
-    int row;
-    int64_t c;
-    load(p, v, row, c);
-    account(v, row);
+    int row = 0;
+    int64_t c = 0;
+    const bool act = p < npieces;
+    if (act) load(p, v, row, c);
+    account(v, row, act);
   }
   __syncthreads();
   if (tid < 32) {  // nrows ≤ 32: one warp finishes the rows
