@@ -86,31 +86,45 @@ __host__ __device__ __forceinline__ int64_t slice_off(int64_t r, int64_t kb, int
          (kk & 15);
 }
 
-// Slicing: one task = nrows source rows of one operand of one block over the whole K range.
-// Source rows are the rows of op(A) and the columns of op(B) (for ComplexF64 a complex source row
-// of op(A) gives the real row pair 2r, 2r+1). A task is cut into pieces of LK consecutive K
-// values of one source row (LK = 16 real values: one 16-byte slice store; 8 complex values: one
-// 8-byte store per real row and K half), dealt to the threads round-robin:
-//   rows contiguous in memory (real op(A) = A, op(B) = Bᵀ; complex likewise): consecutive
-//     threads take consecutive rows of one K chunk, so every load instruction of a warp reads
-//     consecutive rows (coalesced);
-//   K contiguous (op(A) = Aᵀ/Aᴴ, op(B) = B): consecutive threads take consecutive K chunks of
-//     one row; a thread reads its chunk as 16-byte vectors when the row is aligned.
-// Phase 1 loads the pieces, reduces each piece's maximum magnitude and sum of squares and
-// combines them per row in shared memory; the first kSliceKeep pieces of every thread stay in
-// registers, so tasks with at most kSliceKeep pieces per thread (the planner sizes them so) read
-// the operand once. Phase 2 turns the row maxima into exponents and writes the S slices of every
-// piece.
-struct SliceTask {  // one entry per task
+// Slicing: one task = nrows source rows of one operand of one block over the whole K range, run
+// by one warp. Source rows are the rows of op(A) and the columns of op(B) (for ComplexF64 a
+// complex source row of op(A) gives the real row pair 2r, 2r+1). A row is cut into pieces of LK
+// consecutive K values (LK = 16 real values: one 16-byte slice store; 8 complex values: one
+// 8-byte store per real row and K half). The warp's lanes form R rows × G piece groups
+// (lane = g·R + r): lane (g, r) takes the pieces g, g+G, … of row r of the current R rows.
+//   rows contiguous in memory (real op(A) = A, op(B) = Bᵀ; complex likewise): R ≥ 8, so every
+//     load instruction reads R consecutive rows (64 bytes and more);
+//   K contiguous (op(A) = Aᵀ/Aᴴ, op(B) = B): a lane reads its pieces as 16-byte vectors when the
+//     row is aligned; G covers the row's pieces (R = 1 for rows of 32 pieces and more).
+// Pass 1 reduces every row's largest magnitude and sum of squares (shuffles over the G lanes of
+// the row) and sets the row exponent; pass 2 reads the pieces again (from L2) and writes the S
+// slices. The warp then publishes its rows to the products through the readiness counts.
+struct SliceTask {  // one entry per task, with every block field the task needs (one load round)
+  int64_t xoff;     // element offset of source row 0 in A or B
+  int64_t rs, ks;   // source row and K strides in elements
+  int64_t ws_s;     // workspace byte offset of the operand's slices
+  int64_t ws_e;     // workspace byte offset of the operand's row exponents
   int32_t block;
   int32_t operand;  // 0 = rows of op(A), 1 = columns of op(B)
   int32_t r0;       // first source row
-  int32_t nrows;    // source rows of the task (≤ kSliceMaxRows)
+  int32_t nrows;    // source rows of the task
+  int32_t msrc;     // source rows of the operand
+  int32_t k;        // K of the block (source values per row)
+  int32_t kpad;     // padded K of the slices
+  int32_t conj;     // 1: conjugate the values (op = C)
 };
 
-constexpr int kSlicePlanThreads = 256;  // threads the planner sizes the tasks for (at least)
-constexpr int kSliceKeep = 2;           // pieces per thread held in registers between the phases
-constexpr int kSliceMaxRows = 32;       // source rows per task
+constexpr int kTaskPieces = 32;  // pieces per slicing task the planner aims at (one pass of a warp)
+
+// piece groups G of a slicing warp (rows per pass R = 32 / G): the smallest power of two that
+// leaves every lane one piece of a row, at most 32 (each pass of the warp is then one load
+// latency for rows of up to 32 pieces, whatever the layout; rows contiguous in memory share their
+// 32-byte sectors with the tasks of the neighbouring rows, which find them in L2)
+__host__ __device__ __forceinline__ int slice_groups(int nchunk) {
+  int g = 1;
+  while (g < nchunk && g < 32) g <<= 1;
+  return g;
+}
 
 template <int LK>
 struct Piece;  // LK int8 digits: one store per slice
@@ -142,8 +156,9 @@ __device__ __forceinline__ double sq_of(double v) { return v * v; }
 __device__ __forceinline__ double sq_of(double2 v) { return fma(v.x, v.x, v.y * v.y); }
 
 // LK consecutive K values c .. c+LK−1 of the source row at element offset `base` (K stride
-// ks), zero beyond ksrc or for an invalid row
-template <bool CPLX, bool ROWC, int LK>
+// ks), zero beyond ksrc or for an invalid row; K-contiguous real rows (ks = 1) are read as 16-byte
+// vectors where the piece is whole and aligned
+template <bool CPLX, int LK>
 __device__ __forceinline__ void load_piece(const typename SrcVal<CPLX>::T *__restrict__ X, int64_t base,
                                            int64_t ks, int64_t c, int64_t ksrc, bool rv,
                                            typename SrcVal<CPLX>::T (&v)[LK]) {
@@ -155,8 +170,8 @@ __device__ __forceinline__ void load_piece(const typename SrcVal<CPLX>::T *__res
     return;
   }
   const T *p = X + base + c * ks;
-  if constexpr (!ROWC && !CPLX) {
-    if (c + LK <= ksrc && (reinterpret_cast<uintptr_t>(p) & 15) == 0) {
+  if constexpr (!CPLX) {
+    if (ks == 1 && c + LK <= ksrc && (reinterpret_cast<uintptr_t>(p) & 15) == 0) {
       const double2 *p2 = reinterpret_cast<const double2 *>(p);
 #pragma unroll
       for (int h = 0; h < LK / 2; ++h) {
@@ -256,7 +271,7 @@ __device__ __forceinline__ void store_piece(const typename SrcVal<CPLX>::T (&v)[
     for (int q = 0; q < LK; ++q) x[q] = to_fixed(v[q], rsc);
     sign_masks([&](int q) { return v[q]; }, M);
     int8_t *p = base + slice_off(r, c, kpad, pr, S);
-#pragma unroll
+#pragma unroll 1
     for (int sl = 0; sl < S; ++sl) *reinterpret_cast<P *>(p + sl * plane) = slice_piece<S, LK>(x, M, sl);
   } else {
     Fixed xr[LK], xi[LK];
@@ -275,7 +290,7 @@ __device__ __forceinline__ void store_piece(const typename SrcVal<CPLX>::T (&v)[
       int8_t *p1 = base + slice_off(2 * r, kfull + c, kpad, pr, S);
       int8_t *p2 = base + slice_off(2 * r + 1, c, kpad, pr, S);
       int8_t *p3 = base + slice_off(2 * r + 1, kfull + c, kpad, pr, S);
-#pragma unroll
+#pragma unroll 1
       for (int sl = 0; sl < S; ++sl) {
         const P ur = slice_piece<S, LK>(xr, Mr, sl);
         const int64_t o = sl * plane;
@@ -287,7 +302,7 @@ __device__ __forceinline__ void store_piece(const typename SrcVal<CPLX>::T (&v)[
     } else {  // column j of op(B): [Re | Im]
       int8_t *p0 = base + slice_off(r, c, kpad, pr, S);
       int8_t *p1 = base + slice_off(r, kfull + c, kpad, pr, S);
-#pragma unroll
+#pragma unroll 1
       for (int sl = 0; sl < S; ++sl) {
         const int64_t o = sl * plane;
         *reinterpret_cast<P *>(p0 + o) = slice_piece<S, LK>(xr, Mr, sl);
@@ -302,126 +317,66 @@ __device__ __forceinline__ void store_piece(const typename SrcVal<CPLX>::T (&v)[
 // row", and the largest row 2-norms as double bits)
 constexpr int kExpBias = 4096;
 
-// Per-row maximum and sum of squares of the lanes of a warp (all lanes call; row −1 = no value).
-// The lanes holding one row form runs of consecutive lanes (a row can recur later in the warp);
-// every run is reduced to its first lane with a windowed shuffle reduction keyed by the run's
-// first lane, and that lane adds the run's values with one shared-memory atomic each.
-__device__ __forceinline__ void warp_row_account(int row, double m, double s2, unsigned long long *rmax, double *rsq) {
-  const unsigned full = 0xffffffffu;
-  const int lane = threadIdx.x & 31;
-  const int rp = __shfl_up_sync(full, row, 1);
-  const bool head = lane == 0 || rp != row;
-  int start = head ? lane : 0;  // first lane of this lane's run: a prefix maximum of the heads
-#pragma unroll
-  for (int d = 1; d < 32; d <<= 1) {
-    const int o = __shfl_up_sync(full, start, d);
-    if (lane >= d) start = max(start, o);
-  }
-#pragma unroll
-  for (int d = 1; d < 32; d <<= 1) {
-    const int so = __shfl_down_sync(full, start, d);
-    const double mo = __shfl_down_sync(full, m, d);
-    const double qo = __shfl_down_sync(full, s2, d);
-    if (lane + d < 32 && so == start) {
-      m = fmax(m, mo);
-      s2 += qo;
-    }
-  }
-  if (head && row >= 0 && m > 0.0) {
-    atomicMax(&rmax[row], (unsigned long long)__double_as_longlong(m));
-    atomicAdd(&rsq[row], s2);
-  }
+__device__ __forceinline__ void fence_proxy_async_global() {
+  asm volatile("fence.proxy.async.global;\n" ::: "memory");
 }
 
-// One slicing task with the NT threads of the CTA. rmax, rsq (zeroed by the caller) and rexp
-// are per-row shared-memory scratch of kSliceMaxRows entries; bst receives the block statistics.
-template <int S, bool CPLX, bool ROWC, int NT>
-__device__ __forceinline__ void slice_task(const GBlock &b, const SliceTask &task, const void *Xv, int8_t *ws,
-                                           unsigned long long *rmax, int *rexp, double *rsq,
-                                           unsigned long long *bst) {
+// One slicing task run by the calling warp (every lane calls): row exponents into the
+// workspace, the S slices of every row, the block statistics into bst. A lane keeps its first
+// piece of a row in registers between the passes; only rows of more than G pieces are read twice
+// (the second time from L2).
+template <int S, bool CPLX>
+__device__ __forceinline__ void slice_warp_task(const SliceTask &task, const void *Xv, int8_t *ws,
+                                                unsigned long long *bst) {
   using T = typename SrcVal<CPLX>::T;
   constexpr int LK = CPLX ? 8 : 16;
-  const int tid = threadIdx.x;
+  const unsigned full = 0xffffffffu;
+  const int lane = threadIdx.x & 31;
   const int op = task.operand;
-  const int opx = op == 0 ? b.opA : b.opB;
-  const int64_t xo = op == 0 ? b.offA : b.offB;
-  // strides of source rows and K in elements
-  int64_t rs, ks;
-  if (op == 0) {
-    rs = opx == TKB_OP_N ? 1 : b.lda;
-    ks = opx == TKB_OP_N ? b.lda : 1;
-  } else {
-    rs = opx == TKB_OP_N ? b.ldb : 1;
-    ks = opx == TKB_OP_N ? 1 : b.ldb;
-  }
-  const bool conj = opx == TKB_OP_C;
-  const int64_t msrc = op == 0 ? b.m : b.n;
-  const int64_t kfull = CPLX ? b.kpad / 2 : b.kpad;
+  const int64_t rs = task.rs, ks = task.ks;
+  const int64_t kfull = CPLX ? task.kpad / 2 : task.kpad;
   const int nchunk = (int)(kfull / LK);
-  const int nrows = task.nrows;
-  const int npieces = nrows * nchunk;
+  const int G = slice_groups(nchunk), R = 32 / G;
+  const int gq = lane / R, rr = lane - gq * R;
+  const bool conj = task.conj != 0;
   const T *X = reinterpret_cast<const T *>(Xv);
-  auto piece_of = [&](int p, int &row, int64_t &c) {
-    if (ROWC) {
-      row = p % nrows;
-      c = (int64_t)(p / nrows) * LK;
-    } else {
-      row = p / nchunk;
-      c = (int64_t)(p % nchunk) * LK;
-    }
-  };
-  auto load = [&](int p, T (&v)[LK], int &row, int64_t &c) {
-    piece_of(p, row, c);
-    const int64_t r = task.r0 + row;
-    load_piece<CPLX, ROWC, LK>(X, xo + r * rs, ks, c, b.k, r < msrc, v);
-  };
-  // a piece's maximum magnitude and sum of squares, combined per row: first over the runs of
-  // lanes of the warp that hold the same row (every lane takes part; lanes without a piece pass
-  // row −1), then one shared-memory atomic per run
-  auto account = [&](const T (&v)[LK], int row, bool active) {
+  int8_t *base = ws + task.ws_s;
+  int32_t *ex = reinterpret_cast<int32_t *>(ws + task.ws_e);
+  unsigned ebm = 0u;  // largest biased exponent of the task's nonzero rows
+  double nrm = 0.0;   // largest 2-norm of the task's rows
+#pragma unroll 1
+  for (int rb = 0; rb < task.nrows; rb += R) {
+    const int64_t r = task.r0 + rb + rr;
+    const bool rv = rb + rr < task.nrows && r < task.msrc;
+    const int64_t rowbase = task.xoff + r * rs;
+    // pass 1: the lane's first piece (kept in registers), then any further pieces; lanes past the
+    // row's last piece (gq ≥ nchunk) hold zeros and store nothing
+    const bool has = rv && gq < nchunk;
+    T v0[LK];
+    load_piece<CPLX, LK>(X, rowbase, ks, (int64_t)gq * LK, task.k, has, v0);
     double m = 0.0, s2 = 0.0;
-    if (active) {
+#pragma unroll
+    for (int l = 0; l < LK; ++l) {
+      m = fmax(m, absmax(v0[l]));
+      s2 += sq_of(v0[l]);
+    }
+#pragma unroll 1
+    for (int c = gq + G; c < nchunk; c += G) {
+      T w[LK];
+      load_piece<CPLX, LK>(X, rowbase, ks, (int64_t)c * LK, task.k, rv, w);
 #pragma unroll
       for (int l = 0; l < LK; ++l) {
-        m = fmax(m, absmax(v[l]));
-        s2 += sq_of(v[l]);
+        m = fmax(m, absmax(w[l]));
+        s2 += sq_of(w[l]);
       }
-    } else {
-      row = -1;
     }
-    warp_row_account(row, m, s2, rmax, rsq);
-  };
-
-  // phase 1: row maxima and sums of squares; the first kSliceKeep pieces stay in registers
-  // (the loops run warp-uniformly: every lane of a warp reaches the warp reductions together)
-  const int wbase = tid & ~31, lane = tid & 31;
-  T keep[kSliceKeep][LK];
-#pragma unroll
-  for (int q = 0; q < kSliceKeep; ++q) {
-    const int p = tid + q * NT;
-    int row = 0;
-    int64_t c = 0;
-    const bool act = p < npieces;
-    if (act) load(p, keep[q], row, c);
-    account(keep[q], row, act);
-  }
-  for (int p0 = wbase + kSliceKeep * NT; p0 < npieces; p0 += NT) {
-    const int p = p0 + lane;
-    T v[LK];
-    int row = 0;
-    int64_t c = 0;
-    const bool act = p < npieces;
-    if (act) load(p, v, row, c);
-    account(v, row, act);
-  }
-  __syncthreads();
-  if (tid < 32) {  // nrows ≤ 32: one warp finishes the rows
-    const int64_t r = task.r0 + tid;
-    const double m = tid < nrows ? __longlong_as_double((long long)rmax[tid]) : 0.0;
+#pragma unroll 1
+    for (int o = R; o < 32; o <<= 1) {
+      m = fmax(m, __shfl_xor_sync(full, m, o));
+      s2 += __shfl_xor_sync(full, s2, o);
+    }
     const int e = row_exponent<S>(m);
-    if (tid < nrows) rexp[tid] = e;
-    if (tid < nrows && r < msrc) {
-      int32_t *ex = reinterpret_cast<int32_t *>(ws + (op == 0 ? b.wsEA : b.wsEB));
+    if (rv && gq == 0) {
       if (CPLX && op == 0) {
         ex[2 * r] = e;
         ex[2 * r + 1] = e;
@@ -429,39 +384,25 @@ __device__ __forceinline__ void slice_task(const GBlock &b, const SliceTask &tas
         ex[r] = e;
       }
     }
-    // block statistics: largest exponent and 2-norm among the task's nonzero rows
-    const unsigned eb = (m > 0.0) ? (unsigned)(e + kExpBias) : 0u;
-    double nrm = (m > 0.0) ? sqrt(rsq[tid]) : 0.0;
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) nrm = fmax(nrm, __shfl_xor_sync(0xffffffffu, nrm, o));
-    const unsigned ebm = __reduce_max_sync(0xffffffffu, eb);
-    if (tid == 0 && ebm != 0u) {
-      atomicMax(&bst[4 * task.block + op], (unsigned long long)ebm);
-      atomicMax(&bst[4 * task.block + 2 + op], (unsigned long long)__double_as_longlong(nrm));
+    if (rv && m > 0.0) {
+      ebm = max(ebm, (unsigned)(e + kExpBias));
+      nrm = fmax(nrm, sqrt(s2));
+    }
+    // pass 2: the slices of the kept piece, then of the further pieces (read again, from L2)
+    if (has) store_piece<S, CPLX, LK>(v0, op, conj, r, (int64_t)gq * LK, kfull, task.kpad, base, e);
+#pragma unroll 1
+    for (int c = gq + G; c < nchunk; c += G) {
+      T w[LK];
+      load_piece<CPLX, LK>(X, rowbase, ks, (int64_t)c * LK, task.k, rv, w);
+      if (rv) store_piece<S, CPLX, LK>(w, op, conj, r, (int64_t)c * LK, kfull, task.kpad, base, e);
     }
   }
-  __syncthreads();
-
-  // phase 2: slices (rows beyond the operand are not written: their outputs are discarded)
-  int8_t *base = ws + (op == 0 ? b.wsA : b.wsB);
+  ebm = __reduce_max_sync(full, ebm);
 #pragma unroll
-  for (int q = 0; q < kSliceKeep; ++q) {
-    const int p = tid + q * NT;
-    if (p < npieces) {
-      int row;
-      int64_t c;
-      piece_of(p, row, c);
-      const int64_t r = task.r0 + row;
-      if (r < msrc) store_piece<S, CPLX, LK>(keep[q], op, conj, r, c, kfull, b.kpad, base, rexp[row]);
-    }
-  }
-  for (int p = tid + kSliceKeep * NT; p < npieces; p += NT) {
-    T v[LK];
-    int row;
-    int64_t c;
-    load(p, v, row, c);
-    const int64_t r = task.r0 + row;
-    if (r < msrc) store_piece<S, CPLX, LK>(v, op, conj, r, c, kfull, b.kpad, base, rexp[row]);
+  for (int o = 16; o > 0; o >>= 1) nrm = fmax(nrm, __shfl_xor_sync(full, nrm, o));
+  if (lane == 0 && ebm != 0u) {
+    atomicMax(&bst[4 * task.block + op], (unsigned long long)ebm);
+    atomicMax(&bst[4 * task.block + 2 + op], (unsigned long long)__double_as_longlong(nrm));
   }
 }
 
@@ -509,6 +450,33 @@ __device__ __forceinline__ uint64_t globaltimer_ns() {
   asm volatile("mov.u64 %0, %%globaltimer;\n" : "=l"(t));
   return t;
 }
+
+// Timeline build (compiled with -DTKB_TIMELINE into a separate library): per CTA, global-timer
+// stamps (ns) at fixed points of the fused kernel, counts, and wait/work time sums, read back
+// with tkb_timeline_read. The default build compiles every stamp away.
+#ifdef TKB_TIMELINE
+constexpr int kTlCtas = 256, kTlSlots = 32;
+__device__ unsigned long long tkb_tl[kTlCtas * kTlSlots];
+#define TL_AT(k) (tkb_tl[blockIdx.x * kTlSlots + (k)])
+#define TL_STAMP(k)                                 \
+  do {                                              \
+    if (blockIdx.x < kTlCtas) TL_AT(k) = globaltimer_ns(); \
+  } while (0)
+#define TL_ADD(k, v)                                                          \
+  do {                                                                        \
+    if (blockIdx.x < kTlCtas) atomicAdd(&TL_AT(k), (unsigned long long)(v)); \
+  } while (0)
+#define TL_MAX(k, v)                                                          \
+  do {                                                                        \
+    if (blockIdx.x < kTlCtas) atomicMax(&TL_AT(k), (unsigned long long)(v)); \
+  } while (0)
+#define TL_NOW() globaltimer_ns()
+#else
+#define TL_MAX(k, v) ((void)0)
+#define TL_STAMP(k) ((void)0)
+#define TL_ADD(k, v) ((void)0)
+#define TL_NOW() 0ull
+#endif
 // bounded wait on a phase parity: false once 2 s of wall time have passed
 __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity) {
   const uint32_t addr = smem_u32(bar);
@@ -629,7 +597,7 @@ __device__ __forceinline__ int choose_slices(const unsigned long long *bst, int 
   const double cmax = 4.5 * na * nb / sqrt(k);
   const int e = (int)ea + (int)eb - 2 * kExpBias;
   for (int s = 3; s <= SM; ++s) {
-    const double est = kGuardSigma * sqrt((double)s * k) * ldexp(1.0, e - 7 * s);
+    const double est = kGuardSigma * sqrt((double)s * k) * scale2(1.0, e - 7 * s);
     if (est <= kSliceTol * kSliceMargin * cmax) return s;
   }
   return 0;
@@ -780,33 +748,19 @@ struct FusedArgs {
   const double *A, *B;
   double *C;
   int8_t *ws;
-  int *cnt;                 // [0] slicing claims, [1] finished CTAs, [2] tiles recomputed in FP64,
-                            // [3 + 2·block + operand] rows sliced, [3 + 2·nblocks + slot] split-K arrivals
+  int *cnt;                 // [0] slicing claims, [1] finished product CTAs, [2] tiles recomputed in
+                            // FP64, [3] finished slicing warps, [4 + slot] split-K arrivals
   unsigned long long *bst;  // 4 per block: statistics of the slicing
   int *slices_out;          // per block: the slice count of the last launch (0 = FP64, −1 = no
                             // products), then the number of tiles the check sent to FP64
-  double *part;             // split-K partial tiles, [col][row] per piece
+  double *part;             // split-K partial tiles, [col][row] per piece, then one hold tile per CTA
+  int hold0;                // index of CTA 0's hold tile in part
   int *err;
   CDbl alpha, beta;
   int nstasks, nitems, nblocks;
   int fixed;                // 1: the caller fixed the slice count (every block uses S, no check)
 };
 
-__device__ __forceinline__ int ld_acquire(const int *p) {
-  int v;
-  asm volatile("ld.acquire.gpu.global.s32 %0, [%1];\n" : "=r"(v) : "l"(p) : "memory");
-  return v;
-}
-// bounded wait until *p ≥ target (acquire at GPU scope); false once 2 s have passed or the CTA
-// aborts
-__device__ __forceinline__ bool wait_at_least(const int *p, int target, const volatile int *abort) {
-  const uint64_t t0 = globaltimer_ns();
-  while (true) {
-    if (ld_acquire(p) >= target) return true;
-    if (*abort || globaltimer_ns() - t0 > 2000000000ull) return false;
-    __nanosleep(64);
-  }
-}
 // bounded mbarrier wait that also gives up when the CTA aborts
 __device__ __forceinline__ bool mbar_wait_abortable(uint64_t *bar, uint32_t parity, const volatile int *abort) {
   const uint32_t addr = smem_u32(bar);
@@ -844,9 +798,6 @@ __device__ __forceinline__ bool epi_any(bool v) {
       : "memory");
   return r != 0;
 }
-__device__ __forceinline__ void fence_proxy_async_global() {
-  asm volatile("fence.proxy.async.global;\n" ::: "memory");
-}
 
 // the exact FP64 value of the first Sb int32 diagonals of one output (Horner in base 128 over
 // three int64 groups, each below 2^46, then scaled and summed in FP64)
@@ -868,23 +819,24 @@ __device__ __forceinline__ double recombine_value(const uint32_t (&r)[S][W], int
   return acc;
 }
 
-// the α/β update and store of 16 values of one row (one column chunk); real or complex rows
+// the α/β update and store of 8 values of one row (columns j0 .. j0+7); real or complex rows
+// (complex: every lane takes part, the partner row comes by shuffle)
 template <bool CPLX>
-__device__ __forceinline__ void store_chunk(const double (&v)[16], int64_t i, int64_t j0, const GBlock &b, double *C,
+__device__ __forceinline__ void store_group(const double (&v)[8], int64_t i, int64_t j0, const GBlock &b, double *C,
                                             CDbl alpha, CDbl beta, bool bz) {
   if constexpr (!CPLX) {
-    const int nj = (int)min((int64_t)16, b.n - j0);
+    const int nj = (int)min((int64_t)8, b.n - j0);
     if (i >= b.m || nj <= 0) return;
     double *pc = C + b.offC + i + j0 * b.ldc;
-    double old[16];
+    double old[8];
 #pragma unroll
-    for (int q = 0; q < 16; ++q) old[q] = (!bz && q < nj) ? pc[q * b.ldc] : 0.0;
+    for (int q = 0; q < 8; ++q) old[q] = (!bz && q < nj) ? pc[q * b.ldc] : 0.0;
 #pragma unroll
-    for (int q = 0; q < 16; ++q)
+    for (int q = 0; q < 8; ++q)
       if (q < nj) pc[q * b.ldc] = bz ? alpha.x * v[q] : fma(beta.x, old[q], alpha.x * v[q]);
   } else {
 #pragma unroll
-    for (int q = 0; q < 16; ++q) store_out(v[q], i, j0 + q, b, 1, C, alpha, beta, bz, 1);
+    for (int q = 0; q < 8; ++q) store_out(v[q], i, j0 + q, b, 1, C, alpha, beta, bz, 1);
   }
 }
 
@@ -901,18 +853,15 @@ __global__ void __launch_bounds__(kFusedThreads, 1) gemm_split_fused_kernel(cons
   uint64_t *acc_empty = acc_full + 1;
   uint64_t *drain = acc_full + 2;
   uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(acc_full + 3);
-  int *claim = reinterpret_cast<int *>(acc_full + 4);  // [0..1] slicing claims (double-buffered), [2] ticket
+  int *claim = reinterpret_cast<int *>(acc_full + 4);  // [2]: split-K arrival ticket
   volatile int *abort = claim + 3;
-  unsigned long long *rmax = reinterpret_cast<unsigned long long *>(acc_full + 6);  // kSliceMaxRows
-  double *rsq = reinterpret_cast<double *>(rmax + kSliceMaxRows);                   // kSliceMaxRows
-  int *rexp = reinterpret_cast<int *>(rsq + kSliceMaxRows);                         // kSliceMaxRows
   // tile check: per epilogue warp, largest |C|, row exponent and column exponent (two buffers)
-  double *gmax = reinterpret_cast<double *>(rexp + kSliceMaxRows);  // [2][kEpiWarps]
+  double *gmax = reinterpret_cast<double *>(acc_full + 6);    // [2][kEpiWarps]
   int *gexp = reinterpret_cast<int *>(gmax + 2 * kEpiWarps);        // [2][kEpiWarps][2]
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const FusedArgs &g = args;
-  int *ready = g.cnt + 3;
-  int *arrive = g.cnt + 3 + 2 * g.nblocks;
+  int *arrive = g.cnt + 4;
+  if (tid == 0) TL_STAMP(0);
 
   if (tid == 0) {
 #pragma unroll
@@ -935,47 +884,13 @@ __global__ void __launch_bounds__(kFusedThreads, 1) gemm_split_fused_kernel(cons
   __syncthreads();
   tc_fence_after();
   const uint32_t tmem = *tmem_slot;
-  pdl_wait();  // operands and C come from earlier kernels of the stream
+  pdl_wait();  // the slicing launch has finished; C comes from earlier kernels of the stream
+  if (tid == 0) TL_STAMP(1);
 
-  // ---- phase 1: slicing tasks, claimed from the device counter ----------------------------
-  if (tid == 0) claim[0] = atomicAdd(&g.cnt[0], 1);
-  __syncthreads();
-  int t = claim[0];
-  for (int it = 0; t < g.nstasks; ++it) {
-    const int nb = (it + 1) & 1;
-    if (tid == 0) claim[nb] = atomicAdd(&g.cnt[0], 1);  // the next claim is in flight meanwhile
-    if (tid < kSliceMaxRows) {
-      rmax[tid] = 0ull;
-      rsq[tid] = 0.0;
-    }
-    const SliceTask task = g.stasks[t];
-    const GBlock &b = g.blocks[task.block];
-    __syncthreads();
-    const int op = task.operand;
-    const int opx = op == 0 ? b.opA : b.opB;
-    const bool rowc = op == 0 ? opx == TKB_OP_N : opx != TKB_OP_N;
-    const void *X = op == 0 ? (const void *)g.A : (const void *)g.B;
-    if (rowc) slice_task<S, CPLX, true, kFusedThreads>(b, task, X, g.ws, rmax, rexp, rsq, g.bst);
-    else slice_task<S, CPLX, false, kFusedThreads>(b, task, X, g.ws, rmax, rexp, rsq, g.bst);
-    // the slices are read by bulk copies (async proxy) of other CTAs: fence, then publish
-    fence_proxy_async_global();
-    __syncthreads();
-    if (tid == 0) {
-      __threadfence();
-      atomicAdd(&ready[2 * task.block + op], task.nrows);
-    }
-    t = claim[nb];
-  }
-
-  // ---- phase 2: products ------------------------------------------------------------------
+  // ---- products ------------------------------------------------------------------
   const int G = gridDim.x;
-  // wait (bounded) until both operands of the item's block are sliced; then its slice count
-  auto block_slices = [&](const GBlock &b, int block, int &sb) -> bool {
-    if (!wait_at_least(&ready[2 * block], (int)b.m, abort) || !wait_at_least(&ready[2 * block + 1], (int)b.n, abort))
-      return false;
-    sb = g.fixed ? S : choose_slices<S>(g.bst, block, b.kpad);
-    return true;
-  };
+  // a block's slice count (0: the block runs in FP64) from the statistics of the slicing launch
+  auto slices_of = [&](int block, int kpad) -> int { return g.fixed ? S : choose_slices<S>(g.bst, block, kpad); };
   if (warp == kProducerWarp) {
     if (lane == 0) {
       int issued = 0, landed = 0;  // stages issued / known to have landed (for the final drain)
@@ -984,12 +899,8 @@ __global__ void __launch_bounds__(kFusedThreads, 1) gemm_split_fused_kernel(cons
         const SplitTile it = g.items[ii];
         if (it.kind != 0) continue;
         const GBlock b = g.blocks[it.block];
-        int sb = 0;
-        if (!block_slices(b, it.block, sb)) {
-          atomicExch(g.err, 3);
-          *abort = 1;
-          break;
-        }
+        const int sb = slices_of(it.block, b.kpad);
+        if (issued == 0) TL_STAMP(7);
         if (sb == 0) continue;  // the block runs in FP64
         fence_proxy_async_global();
         const int8_t *gA = g.ws + b.wsA + (int64_t)(it.m0 / PANEL_A) * S * PANEL_A * b.kpad;
@@ -998,7 +909,10 @@ __global__ void __launch_bounds__(kFusedThreads, 1) gemm_split_fused_kernel(cons
         for (int kt = it.kb; kt < it.ke; ++kt, ++gs) {
           const int st = gs % NSTAGE, n = gs / NSTAGE;
           if (n > 0) {
-            if (!mbar_wait_abortable(&empty[st], (n - 1) & 1, abort)) {
+            [[maybe_unused]] const unsigned long long te = TL_NOW();
+            const bool waited = mbar_wait_abortable(&empty[st], (n - 1) & 1, abort);
+            TL_ADD(26, TL_NOW() - te);
+            if (!waited) {
               atomicExch(g.err, 1);
               *abort = 1;
               ok = false;
@@ -1015,6 +929,7 @@ __global__ void __launch_bounds__(kFusedThreads, 1) gemm_split_fused_kernel(cons
         }
         if (!ok) break;
       }
+      TL_STAMP(8);
       // every bulk copy must land before the CTA can exit (bounded)
       for (int k = landed; k < issued; ++k) mbar_wait(&full[k % NSTAGE], (k / NSTAGE) & 1);
     }
@@ -1026,13 +941,7 @@ __global__ void __launch_bounds__(kFusedThreads, 1) gemm_split_fused_kernel(cons
       for (int ii = blockIdx.x; ii < g.nitems && ok && !*abort; ii += G) {
         const SplitTile it = g.items[ii];
         if (it.kind != 0) continue;
-        const GBlock b = g.blocks[it.block];
-        int sb = 0;
-        if (!block_slices(b, it.block, sb)) {
-          atomicExch(g.err, 3);
-          *abort = 1;
-          break;
-        }
+        const int sb = slices_of(it.block, g.blocks[it.block].kpad);
         if (sb == 0) continue;
         if (li > 0 && !mbar_wait_abortable(acc_empty, (li - 1) & 1, abort)) {
           atomicExch(g.err, 2);
@@ -1043,7 +952,10 @@ __global__ void __launch_bounds__(kFusedThreads, 1) gemm_split_fused_kernel(cons
         const uint32_t ring0 = smem_u32(smem);
         for (int kt = it.kb; kt < it.ke; ++kt, ++gs) {
           const int st = gs % NSTAGE;
-          if (!mbar_wait_abortable(&full[st], (gs / NSTAGE) & 1, abort)) {
+          [[maybe_unused]] const unsigned long long tf = TL_NOW();
+          const bool landed = mbar_wait_abortable(&full[st], (gs / NSTAGE) & 1, abort);
+          TL_ADD(25, TL_NOW() - tf);
+          if (!landed) {
             atomicExch(g.err, 1);
             *abort = 1;
             ok = false;
@@ -1054,11 +966,11 @@ __global__ void __launch_bounds__(kFusedThreads, 1) gemm_split_fused_kernel(cons
           // the products (s, t), (s, t+1), … share the A slice s and land in the adjacent
           // diagonals s+t, …; up to four B slices (back to back in the stage) form one N ≤ 256
           // operand
-#pragma unroll
+#pragma unroll 1
           for (int s = 0; s < S; ++s) {
             if (s < sb) {
               const uint64_t ad = umma_desc(a0 + s * A_SLICE, 128, 256);
-#pragma unroll
+#pragma unroll 1
               for (int tt = 0; tt < S - s; tt += kMaxSlicesPerMma) {
                 if (tt < sb - s) {
                   const int nsl = (sb - s - tt) < kMaxSlicesPerMma ? (sb - s - tt) : kMaxSlicesPerMma;
@@ -1072,8 +984,10 @@ __global__ void __launch_bounds__(kFusedThreads, 1) gemm_split_fused_kernel(cons
         }
         if (!ok) break;
         umma_commit(acc_full);
+        if (li == 0) TL_STAMP(9);
         ++li;
       }
+      TL_STAMP(10);
       // every MMA issued by this thread completes before TMEM is released (bounded)
       umma_commit(drain);
       mbar_wait(drain, 0);
@@ -1093,17 +1007,16 @@ __global__ void __launch_bounds__(kFusedThreads, 1) gemm_split_fused_kernel(cons
       const int64_t i = it.m0 + row;
       const bool prod = it.kind == 0;
       bool stop = *abort != 0;
-      int sb = 0;
-      if (prod && !stop) {
-        // lane 0 acquires the readiness counts; __syncwarp orders the other lanes' reads of the
-        // statistics and exponents after that acquire
-        if (lane == 0) stop = !block_slices(b, it.block, sb);
-        __syncwarp();
-        stop = __shfl_sync(0xffffffffu, stop ? 1 : 0, 0) != 0;
-        sb = g.fixed ? S : choose_slices<S>(g.bst, it.block, b.kpad);
-      }
+      const int sb = prod ? slices_of(it.block, b.kpad) : 0;
       const bool mma = prod && sb > 0;  // the tile's products ran on the tensor cores
+      [[maybe_unused]] const unsigned long long ta = TL_NOW();
       if (mma && !stop) stop = !mbar_wait_abortable(acc_full, li & 1, abort);
+      if (tid == 0) {
+        TL_ADD(21, TL_NOW() - ta);
+        if (li == 0 && mma) TL_STAMP(11);
+        TL_ADD(18, 1);
+      }
+      [[maybe_unused]] const unsigned long long tr = TL_NOW();
       if (epi_any(stop)) {  // every epilogue warp leaves the loop here, together
         if (tid == 0) {
           atomicExch(g.err, 2);
@@ -1117,73 +1030,80 @@ __global__ void __launch_bounds__(kFusedThreads, 1) gemm_split_fused_kernel(cons
         continue;
       }
       const bool split = it.nsplit > 1;
-      double v[2][16];
-#pragma unroll
-      for (int cc = 0; cc < 2; ++cc)
-#pragma unroll
-        for (int q = 0; q < 16; ++q) v[cc][q] = 0.0;
-      double vmax = 0.0;    // largest |C| of the thread's values (stored already: β = 0, unsplit)
-      int ei = 0, ejm = 0;  // the thread's row exponent, the largest column exponent of its chunks
+      // direct: β = 0 and one piece, so the values go to C as they are recombined (a tile the
+      // check sends to FP64 is overwritten). Otherwise they go to a scratch tile ([col][row]) first:
+      // this piece's partial (split), or the CTA's hold tile (β ≠ 0: C keeps its old values until
+      // the tile check has passed).
+      const bool direct = BZ && !split;
+      double *scr = g.part + (int64_t)(split ? it.pbase + it.sid : g.hold0 + (int)blockIdx.x) * (64 * 128);
+      double vmax = 0.0;    // largest |C| of the thread's values
+      int ei = 0, ejm = 0;  // the thread's row exponent, the largest column exponent of its columns
       if (mma) {
         tc_fence_after();
         const int32_t *eA = reinterpret_cast<const int32_t *>(g.ws + b.wsEA);
         const int32_t *eB = reinterpret_cast<const int32_t *>(g.ws + b.wsEB);
-        ei = i < Mreal ? max(eA[i], -1100) : -1100;
+        // rows past the block (and columns, below) get exponent −1100 and scale 0: their values
+        // become zero and are never stored
+        const bool rok = i < Mreal;
+        ei = rok ? max(eA[i], -1100) : -1100;
         const double rscale = (ei >= -1022 && ei <= 1023) ? pow2i(ei) : 0.0;
-        ejm = -1100;
-#pragma unroll
-        for (int cc = 0; cc < 2; ++cc) {
-          const int c = 2 * half + cc;
-          // this lane's column of the chunk: exponent and scale, shared with the warp by shuffles
-          const int64_t jl = it.n0 + c * 16 + (lane & 15);
-          const int ej = jl < b.n ? max(eB[jl], -1100) : -1100;
-          ejm = max(ejm, ej);
-          const double cs = (ej >= -1022 && ej <= 1023) ? pow2i(ej) : 0.0;
-          // the chunk in two halves of 8 columns (fewer live registers); after the last load of
-          // the second chunk the accumulators go back to the MMA warp
-#pragma unroll
-          for (int hh = 0; hh < 2; ++hh) {
+        // lane l holds the exponent and scale of the warp's column 32·half + l (shared by shuffles)
+        const int64_t jl = it.n0 + 32 * half + lane;
+        const bool cok = jl < b.n;
+        const int ej = cok ? max(eB[jl], -1100) : -1100;
+        const double cs = (ej >= -1022 && ej <= 1023) ? pow2i(ej) : 0.0;
+        ejm = ej;
+        // the exact (ldexp) scaling only where a real row's or column's 2^e is not a normal double
+        const bool slow = __any_sync(0xffffffffu, (rok && rscale == 0.0) || (cok && cs == 0.0));
+        // the warp's 32 columns, 8 at a time (a runtime loop: the code stays small); after the
+        // last group's loads the accumulators go back to the MMA warp
+#pragma unroll 1
+        for (int g8 = 0; g8 < 4; ++g8) {
+          const int c0 = 32 * half + 8 * g8;
+          double w[8];
+          {
             uint32_t r[S][8];
 #pragma unroll
             for (int d = 0; d < S; ++d)
-              if (d < sb)
-                tmem_ld8_issue(tmem + ((uint32_t)(32 * quarter) << 16) + (uint32_t)(d * 64 + c * 16 + hh * 8), r[d]);
+              if (d < sb) tmem_ld8_issue(tmem + ((uint32_t)(32 * quarter) << 16) + (uint32_t)(d * 64 + c0), r[d]);
 #pragma unroll
             for (int d = 0; d < S; ++d)
               if (d < sb) tmem_ld_wait8(r[d]);
-            if (cc == 1 && hh == 1) {
+            if (g8 == 3) {
               tc_fence_before();
               __syncwarp();
               if (lane == 0) mbar_arrive(acc_empty);
             }
 #pragma unroll
-            for (int q = 0; q < 8; ++q) v[cc][hh * 8 + q] = recombine_value<S, 8>(r, q, sb);
+            for (int q = 0; q < 8; ++q) w[q] = recombine_value<S, 8>(r, q, sb);
           }
-          const bool slow = __any_sync(0xffffffffu, rscale == 0.0 || cs == 0.0);
 #pragma unroll
-          for (int q = 0; q < 16; ++q) {
-            const int ejq = __shfl_sync(0xffffffffu, ej, q);
-            const double csq = __shfl_sync(0xffffffffu, cs, q);
-            v[cc][q] = slow ? scale2(v[cc][q], ei + ejq) : v[cc][q] * rscale * csq;
+          for (int q = 0; q < 8; ++q) {
+            const int ejq = __shfl_sync(0xffffffffu, ej, 8 * g8 + q);
+            const double csq = __shfl_sync(0xffffffffu, cs, 8 * g8 + q);
+            w[q] = slow ? scale2(w[q], ei + ejq) : w[q] * rscale * csq;
+            vmax = fmax(vmax, fabs(w[q]));
           }
-          if (BZ && !split) {
-            // β = 0: store at once (no old value of C is needed should the tile check send the
-            // tile to FP64, which then overwrites it), keep only the largest magnitude
+          if (direct) {
+            store_group<CPLX>(w, i, it.n0 + c0, b, g.C, g.alpha, g.beta, true);
+          } else {
 #pragma unroll
-            for (int q = 0; q < 16; ++q) vmax = fmax(vmax, fabs(v[cc][q]));
-            store_chunk<CPLX>(v[cc], i, it.n0 + c * 16, b, g.C, g.alpha, g.beta, true);
+            for (int q = 0; q < 8; ++q) __stcg(&scr[(c0 + q) * 128 + row], w[q]);
           }
+          if (tid == 0 && li == 0 && g8 == 0) TL_STAMP(13);
+        }
+        if (tid == 0) {
+          if (li == 0) TL_STAMP(12);
+          TL_ADD(22, TL_NOW() - tr);
         }
         ++li;
       }
+      [[maybe_unused]] const unsigned long long ts = TL_NOW();
       bool final_piece = true;
       if (split) {
-        // store this piece's partial and count it; the last piece adds all partials in piece order
-        double *mine = g.part + (int64_t)(it.pbase + it.sid) * (64 * 128);
-#pragma unroll
-        for (int cc = 0; cc < 2; ++cc)
-#pragma unroll
-          for (int q = 0; q < 16; ++q) __stcg(&mine[((2 * half + cc) * 16 + q) * 128 + row], v[cc][q]);
+        if (tid == 0) TL_ADD(19, 1);
+        // count this piece (its partial is stored); the last piece adds all partials in piece
+        // order into its own partial tile
         __threadfence();
         epi_sync();
         if (tid == 0) claim[2] = atomicAdd(&arrive[it.slot], 1);
@@ -1192,37 +1112,41 @@ __global__ void __launch_bounds__(kFusedThreads, 1) gemm_split_fused_kernel(cons
         epi_sync();  // the ticket slot is rewritten by the next item
         if (final_piece) {
           __threadfence();
+          // the thread's 32 values of every piece are loaded together (one latency per piece)
+          double v[32];
 #pragma unroll
-          for (int cc = 0; cc < 2; ++cc)
-#pragma unroll
-            for (int q = 0; q < 16; ++q) v[cc][q] = 0.0;
+          for (int q = 0; q < 32; ++q) v[q] = 0.0;
 #pragma unroll 1
           for (int sp = 0; sp < it.nsplit; ++sp) {
-            const double *src = g.part + (int64_t)(it.pbase + sp) * (64 * 128);
+            const double *src = g.part + (int64_t)(it.pbase + sp) * (64 * 128) + (32 * half) * 128 + row;
 #pragma unroll
-            for (int cc = 0; cc < 2; ++cc)
-#pragma unroll
-              for (int q = 0; q < 16; ++q) v[cc][q] += __ldcg(&src[((2 * half + cc) * 16 + q) * 128 + row]);
+            for (int q = 0; q < 32; ++q) v[q] += __ldcg(&src[q * 128]);
           }
-          if (tid == 0) arrive[it.slot] = 0;  // every piece has arrived: free for the next launch
+          vmax = 0.0;
+#pragma unroll
+          for (int q = 0; q < 32; ++q) {
+            vmax = fmax(vmax, fabs(v[q]));
+            __stcg(&scr[(32 * half + q) * 128 + row], v[q]);
+          }
+          if (tid == 0) {
+            arrive[it.slot] = 0;  // every piece has arrived: free for the next launch
+            TL_ADD(20, 1);
+          }
         }
       }
+      if (tid == 0) TL_ADD(23, TL_NOW() - ts);
       if (!final_piece) continue;  // uniform: every epilogue thread read the same ticket
       if (!mma) {                  // β-scale only (k = 0)
-#pragma unroll
-        for (int cc = 0; cc < 2; ++cc)
-          store_chunk<CPLX>(v[cc], i, it.n0 + (2 * half + cc) * 16, b, g.C, g.alpha, g.beta, bz);
+#pragma unroll 1
+        for (int g8 = 0; g8 < 4; ++g8) {
+          const double w[8] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+          store_group<CPLX>(w, i, it.n0 + 32 * half + 8 * g8, b, g.C, g.alpha, g.beta, bz);
+        }
         continue;
       }
       // tile check: largest |C| and exponents of the tile against the error estimate
-      const bool stored = BZ && !split;
+      [[maybe_unused]] const unsigned long long tg = TL_NOW();
       double vm = vmax;
-      if (!stored) {
-#pragma unroll
-        for (int cc = 0; cc < 2; ++cc)
-#pragma unroll
-          for (int q = 0; q < 16; ++q) vm = fmax(vm, fabs(v[cc][q]));
-      }
 #pragma unroll
       for (int o = 16; o > 0; o >>= 1) vm = fmax(vm, __shfl_xor_sync(0xffffffffu, vm, o));
       const int eim = (int)__reduce_max_sync(0xffffffffu, (unsigned)(ei + kExpBias)) - kExpBias;
@@ -1243,47 +1167,90 @@ __global__ void __launch_bounds__(kFusedThreads, 1) gemm_split_fused_kernel(cons
         tf = max(tf, gexp[(buf * kEpiWarps + w) * 2 + 1]);
       }
       ++gi;
-      const double est = kGuardSigma * sqrt((double)sb * (double)b.kpad) * ldexp(1.0, te + tf - 7 * sb);
+      const double est = kGuardSigma * sqrt((double)sb * (double)b.kpad) * scale2(1.0, te + tf - 7 * sb);
       if (!g.fixed && est > kSliceTol * tmax) {  // uniform over the epilogue warps
         if (tid == 0) atomicAdd(&g.cnt[2], 1);
-        if (stored) epi_sync();  // every approximate value of the tile is stored before the overwrite
+        if (direct) epi_sync();  // every approximate value of the tile is stored before the overwrite
         fp64_tile<CPLX>(b, it.m0, it.n0, g.A, g.B, g.C, g.alpha, g.beta, bz, warp, lane);
         continue;
       }
-      if (!stored) {
+      if (!direct) {
+        // the checked values from the scratch tile (written by this thread) to C
+#pragma unroll 1
+        for (int g8 = 0; g8 < 4; ++g8) {
+          const int c0 = 32 * half + 8 * g8;
+          double w[8];
 #pragma unroll
-        for (int cc = 0; cc < 2; ++cc)
-          store_chunk<CPLX>(v[cc], i, it.n0 + (2 * half + cc) * 16, b, g.C, g.alpha, g.beta, bz);
+          for (int q = 0; q < 8; ++q) w[q] = __ldcg(&scr[(c0 + q) * 128 + row]);
+          store_group<CPLX>(w, i, it.n0 + c0, b, g.C, g.alpha, g.beta, bz);
+        }
       }
+      if (tid == 0) TL_ADD(24, TL_NOW() - tg);
     }
+    if (tid == 0) TL_STAMP(16);
   }
 
   // ---- teardown ----------------------------------------------------------------------------
   tc_fence_before();
   __syncthreads();
+  if (tid == 0) TL_STAMP(17);
   if (warp == kMmaWarp) {
     tc_fence_after();
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(kTmemCols));
   }
-  if (tid == 0) {
-    // the last CTA out records the launch's slice counts and checks, and clears the counters
-    __threadfence();
-    if (atomicAdd(&g.cnt[1], 1) == (int)gridDim.x - 1) {
+  if (warp == 0) {
+    // the last CTA out records the launch's slice counts and checks and clears the statistics and
+    // counts for the next launch (its first warp, one block per lane)
+    int last = 0;
+    if (lane == 0) {
       __threadfence();
-      for (int q = 0; q < g.nblocks; ++q) {
+      last = atomicAdd(&g.cnt[1], 1) == (int)gridDim.x - 1;
+    }
+    if (__shfl_sync(0xffffffffu, last, 0)) {
+      __threadfence();
+      for (int q = lane; q < g.nblocks; q += 32) {
         const GBlock &b = g.blocks[q];
         g.slices_out[q] = (b.m > 0 && b.n > 0 && b.k > 0 && !b.skinny) ? (g.fixed ? S : choose_slices<S>(g.bst, q, b.kpad))
                                                                         : -1;
       }
-      g.slices_out[g.nblocks] = g.cnt[2];
-      g.cnt[0] = 0;
-      g.cnt[2] = 0;
-      for (int q = 0; q < 2 * g.nblocks; ++q) ready[q] = 0;
-      for (int q = 0; q < 4 * g.nblocks; ++q) g.bst[q] = 0ull;
-      __threadfence();
-      g.cnt[1] = 0;
+      __syncwarp();
+      for (int q = lane; q < 4 * g.nblocks; q += 32) g.bst[q] = 0ull;
+      if (lane == 0) {
+        g.slices_out[g.nblocks] = g.cnt[2];
+        g.cnt[2] = 0;
+        __threadfence();
+        g.cnt[1] = 0;
+      }
     }
   }
+}
+
+// The slicing launch: warp w of the grid takes the tasks w, w + W, w + 2W, … (W warps; the
+// planner sorts the tasks largest first). Many warps per SM keep many piece loads in flight. It
+// lets the products launch start its prologue as soon as all its CTAs run; that launch waits for
+// it to finish before its first product.
+constexpr int kSliceThreads = 256;
+template <int S, bool CPLX>
+__global__ void __launch_bounds__(kSliceThreads, 2) gemm_split_slice_kernel(const FusedArgs args) {
+  const FusedArgs &g = args;
+  pdl_wait();     // the operands come from earlier kernels of the stream
+  pdl_trigger();  // the products launch may begin its prologue
+  const int lane = threadIdx.x & 31;
+  if (threadIdx.x == 0) TL_STAMP(28);
+  const int nw = (int)gridDim.x * (kSliceThreads / 32);
+  for (int t = (int)blockIdx.x * (kSliceThreads / 32) + (int)(threadIdx.x >> 5); t < g.nstasks; t += nw) {
+    const SliceTask task = g.stasks[t];
+    const void *X = task.operand == 0 ? (const void *)g.A : (const void *)g.B;
+    [[maybe_unused]] const unsigned long long t0 = TL_NOW();
+    slice_warp_task<S, CPLX>(task, X, g.ws, g.bst);
+    if (lane == 0) {
+      TL_ADD(30, 1);
+      TL_MAX(31, TL_NOW() - t0);
+    }
+  }
+  // the slices are read by bulk copies (async proxy) of the products launch
+  fence_proxy_async_global();
+  if (lane == 0) TL_MAX(29, TL_NOW());
 }
 
 size_t tc_smem_bytes(int S) { return ring_stages(S) * (size_t)S * (PANEL_A + PANEL_B) * KSTAGE + kSmemTail; }
@@ -1303,6 +1270,7 @@ int launch_split(tkb_ctx *ctx, const tkb_plan *p, void *C, const void *A, const 
   fa.bst = p->bstat;
   fa.slices_out = p->bslices;
   fa.part = p->part;
+  fa.hold0 = p->part_hold0;
   fa.err = ctx->counters + 8;
   fa.alpha = a;
   fa.beta = b;
@@ -1315,6 +1283,13 @@ int launch_split(tkb_ctx *ctx, const tkb_plan *p, void *C, const void *A, const 
   auto k = cplx ? (bz ? gemm_split_fused_kernel<S, true, true> : gemm_split_fused_kernel<S, true, false>)
                 : (bz ? gemm_split_fused_kernel<S, false, true> : gemm_split_fused_kernel<S, false, false>);
   TKB_CUDA_TRY(ctx, cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  if (fa.nstasks > 0) {
+    auto ks = cplx ? gemm_split_slice_kernel<S, true> : gemm_split_slice_kernel<S, false>;
+    const int warps = kSliceThreads / 32;
+    const int grid = std::max(1, std::min(2 * ctx->num_sms, (fa.nstasks + warps - 1) / warps));
+    TKB_CUDA_TRY(ctx, launch_pdl(ks, dim3((unsigned)grid), dim3(kSliceThreads), 0, ctx->stream, fa));
+    ctx->launches++;
+  }
   TKB_CUDA_TRY(ctx, launch_pdl(k, dim3((unsigned)ctx->num_sms), dim3(kFusedThreads), smem, ctx->stream, fa));
   ctx->launches++;
   TKB_CUDA_TRY(ctx, cudaGetLastError());
@@ -1324,6 +1299,15 @@ int launch_split(tkb_ctx *ctx, const tkb_plan *p, void *C, const void *A, const 
 int64_t roundup(int64_t x, int64_t m) { return (x + m - 1) / m * m; }
 
 }  // namespace
+
+#ifdef TKB_TIMELINE
+// copies the timeline of the last fused launch (kTlCtas × kTlSlots values) and clears it
+extern "C" int tkb_timeline_read(unsigned long long *out) {
+  if (cudaMemcpyFromSymbol(out, tkb_tl, sizeof(tkb_tl)) != cudaSuccess) return -1;
+  static unsigned long long zero[kTlCtas * kTlSlots];
+  return cudaMemcpyToSymbol(tkb_tl, zero, sizeof(tkb_tl)) == cudaSuccess ? kTlSlots : -1;
+}
+#endif
 
 int tkb_gemm_split_prepare(tkb_ctx *ctx, tkb_plan *p) {
   const bool cplx = p->dtype == TKB_C128;
@@ -1362,21 +1346,27 @@ int tkb_gemm_split_prepare(tkb_ctx *ctx, tkb_plan *p) {
     for (int64_t m0 = 0; m0 < M; m0 += PANEL_A)
       for (int64_t n0 = 0; n0 < b.n; n0 += PANEL_B) tiles.push_back({(int32_t)bi, (int32_t)m0, (int32_t)n0, kind});
   }
-  // slicing tasks: as many source rows per task as keep every thread's pieces in registers
-  // (kSliceKeep pieces of kSlicePlanThreads threads; at most kSliceMaxRows rows), halved while
-  // there would be fewer tasks than SMs. Only the operands' own rows are sliced: padding rows of a
-  // panel feed output rows and columns that are never stored.
+  // slicing tasks (one warp each): about kTaskPieces pieces of whole rows, in multiples of the
+  // rows one pass of the warp takes, halved while there would be fewer than 16 tasks per SM. Only the operands' own rows are sliced: padding rows of a panel
+  // feed output rows and columns that are never stored.
   std::vector<SliceTask> jobs;
   if (!sj.empty()) {
     for (int div = 1;; div *= 2) {
       jobs.clear();
       for (const SJob &t : sj) {
-        const int64_t rt =
-            std::min<int64_t>(kSliceMaxRows, std::max<int64_t>(1, (int64_t)kSliceKeep * kSlicePlanThreads / t.nchunk));
-        const int32_t r = (int32_t)std::max<int64_t>(1, rt / div);
-        for (int32_t r0 = 0; r0 < t.nsrc; r0 += r) jobs.push_back({t.block, t.op, r0, std::min(r, t.nsrc - r0)});
+        const int64_t R = 32 / slice_groups(t.nchunk);
+        const int64_t passes = std::max<int64_t>(1, kTaskPieces / (R * std::max<int32_t>(1, t.nchunk)) / div);
+        const int32_t r = (int32_t)(R * passes);
+        for (int32_t r0 = 0; r0 < t.nsrc; r0 += r) {
+          SliceTask j{};
+          j.block = t.block;
+          j.operand = t.op;
+          j.r0 = r0;
+          j.nrows = std::min(r, t.nsrc - r0);
+          jobs.push_back(j);
+        }
       }
-      if ((int64_t)jobs.size() >= ctx->num_sms || div >= 8) break;
+      if ((int64_t)jobs.size() >= 16 * (int64_t)ctx->num_sms || div >= 64) break;
     }
     // the tasks with the most pieces first
     std::vector<int32_t> nch(p->hblocks.size(), 0);
@@ -1396,6 +1386,29 @@ int tkb_gemm_split_prepare(tkb_ctx *ctx, tkb_plan *p) {
     off += (size_t)b.npad * 4;
   }
   p->expo_bytes = (int64_t)off - p->expo_off;
+  // the block fields every slicing task needs, in its own record
+  for (SliceTask &j : jobs) {
+    const GBlock &b = p->hblocks[j.block];
+    const int opx = j.operand == 0 ? b.opA : b.opB;
+    if (j.operand == 0) {
+      j.xoff = b.offA;
+      j.rs = opx == TKB_OP_N ? 1 : b.lda;
+      j.ks = opx == TKB_OP_N ? b.lda : 1;
+      j.ws_s = b.wsA;
+      j.ws_e = b.wsEA;
+      j.msrc = (int32_t)b.m;
+    } else {
+      j.xoff = b.offB;
+      j.rs = opx == TKB_OP_N ? b.ldb : 1;
+      j.ks = opx == TKB_OP_N ? 1 : b.ldb;
+      j.ws_s = b.wsB;
+      j.ws_e = b.wsEB;
+      j.msrc = (int32_t)b.n;
+    }
+    j.k = (int32_t)b.k;
+    j.kpad = b.kpad;
+    j.conj = opx == TKB_OP_C ? 1 : 0;
+  }
   off = roundup((int64_t)off, 256);
   std::stable_sort(tiles.begin(), tiles.end(), [&](const GTile &x, const GTile &y) {
     return p->hblocks[x.block].kpad > p->hblocks[y.block].kpad;
@@ -1458,12 +1471,15 @@ int tkb_gemm_split_prepare(tkb_ctx *ctx, tkb_plan *p) {
     e = cudaMalloc(&p->kstiles, kt.size() * sizeof(SplitTile));
     if (e == cudaSuccess) e = cudaMemcpy(p->kstiles, kt.data(), kt.size() * sizeof(SplitTile), cudaMemcpyHostToDevice);
   }
-  if (e == cudaSuccess && nslots > 0)
-    e = cudaMalloc((void **)&p->part, (size_t)npart * 64 * 128 * sizeof(double));
-  // claim, finish and check counts, readiness counts, then one split-K arrival counter per split
+  // the partial tiles of the split items, then one hold tile per CTA (β ≠ 0: the recombined
+  // values wait there for the tile check)
+  p->part_hold0 = npart;
+  if (e == cudaSuccess && !kt.empty())
+    e = cudaMalloc((void **)&p->part, (size_t)(npart + ctx->num_sms) * 64 * 128 * sizeof(double));
+  // claim, finish, check and slicing-warp counts, then one split-K arrival counter per split
   // tile; the block statistics; the per-block slice counts of the last launch
   const size_t nb = p->hblocks.size();
-  const size_t ncnt = 3 + 2 * nb + (size_t)nslots;
+  const size_t ncnt = 4 + (size_t)nslots;
   if (e == cudaSuccess) e = cudaMalloc((void **)&p->pcnt, ncnt * sizeof(int));
   if (e == cudaSuccess) e = cudaMemset(p->pcnt, 0, ncnt * sizeof(int));
   if (e == cudaSuccess) e = cudaMalloc((void **)&p->bstat, std::max<size_t>(1, 4 * nb) * sizeof(unsigned long long));

@@ -214,6 +214,7 @@ struct tkb_plan {
   int64_t nptasks = 0;
   int pgrid = 0;                // CTAs of the plain launch
   double *part = nullptr;       // split-K FP64 partial tiles (rewritten every launch)
+  int32_t part_hold0 = 0;       // split: first of the per-CTA hold tiles in `part` (after the partials)
   int *pcnt = nullptr;          // device counters (split-K arrivals; split: claims and readiness too), self-clearing
   unsigned long long *bstat = nullptr;  // split: per-block statistics of the slicing (self-clearing)
   int32_t *bslices = nullptr;   // split: slice count per block of the last launch, then the FP64-checked tiles

@@ -26,18 +26,21 @@ def sources():
         os.path.join(os.path.dirname(ROOT), "include", "tkb200.h")]
 
 
-def build(force: bool = False, verbose: bool = False) -> str:
-    """Compile every translation unit in parallel (one nvcc per file), then link the .so."""
+def build(force: bool = False, verbose: bool = False, timeline: bool = False) -> str:
+    """Compile every translation unit in parallel (one nvcc per file), then link the .so.
+
+    timeline: build libtkb200_timeline.so instead, with the fused split kernel's global-timer
+    stamps compiled in (read back with tkb_timeline_read); the default library has none."""
     from concurrent.futures import ThreadPoolExecutor
     os.makedirs(LIBDIR, exist_ok=True)
-    out = os.path.join(LIBDIR, "libtkb200.so")
+    out = os.path.join(LIBDIR, "libtkb200_timeline.so" if timeline else "libtkb200.so")
     if not force and os.path.exists(out):
         newest = max(os.path.getmtime(s) for s in sources())
         if os.path.getmtime(out) >= newest:
             return out
-    objdir = os.path.join(LIBDIR, "obj")
+    objdir = os.path.join(LIBDIR, "obj_timeline" if timeline else "obj")
     os.makedirs(objdir, exist_ok=True)
-    compile_flags = [f for f in NVCC_FLAGS if f != "-shared"]
+    compile_flags = [f for f in NVCC_FLAGS if f != "-shared"] + (["-DTKB_TIMELINE"] if timeline else [])
 
     def compile_one(src):
         obj = os.path.join(objdir, os.path.splitext(src)[0] + ".o")
@@ -57,4 +60,4 @@ def build(force: bool = False, verbose: bool = False) -> str:
 
 
 if __name__ == "__main__":
-    print(build(force="--force" in sys.argv, verbose=True))
+    print(build(force="--force" in sys.argv, verbose=True, timeline="--timeline" in sys.argv))
