@@ -70,11 +70,6 @@ __device__ __noinline__ double ldexp_slow(double v, int e) { return ldexp(v, e);
 __device__ __forceinline__ double scale2(double v, int e) {
   return (e >= -1022 && e <= 1023) ? v * pow2i(e) : ldexp_slow(v, e);
 }
-// exact int64 → double for |x| < 2^51: x is added to the mantissa of 1.5·2^52 (whose unit in
-// the last place is 1), and 1.5·2^52 is subtracted again
-__device__ __forceinline__ double i2d_small(int64_t x) {
-  return __longlong_as_double(x + 0x4338000000000000ll) - 6755399441055744.0;
-}
 
 // byte offset of (slice 0, row r, K byte kb) in a block's slices (pr: rows per panel, 64 or
 // 128); slice s is s·pr·KSTAGE bytes further
@@ -799,23 +794,20 @@ __device__ __forceinline__ bool epi_any(bool v) {
   return r != 0;
 }
 
-// the exact FP64 value of the first Sb int32 diagonals of one output (Horner in base 128 over
-// three int64 groups, each below 2^46, then scaled and summed in FP64)
+// exact int32 → double without a conversion instruction: the bits 0x43300000:(x ^ 2^31) are the
+// double 2^52 + 2^31 + x, from which 2^52 + 2^31 is subtracted exactly
+__device__ __forceinline__ double i32_to_f64(uint32_t x) {
+  return __hiloint2double(0x43300000, (int)(x ^ 0x80000000u)) - 4503601774854144.0;
+}
+// the first Sb int32 diagonals of one output combined in FP64, times 2^(7(Sb+1)): Horner in base
+// 128 (every diagonal converts exactly; once the partial sum passes 2^53 each fused multiply-add
+// rounds, a relative error of a few 2^-53 of the diagonals' scale, far below the truncation)
 template <int S, int W>
 __device__ __forceinline__ double recombine_value(const uint32_t (&r)[S][W], int q, int Sb) {
-  int64_t g0 = 0, g1 = 0, g2 = 0;
+  double acc = i32_to_f64(r[0][q]);
 #pragma unroll
-  for (int d = 0; d < S; ++d) {
-    if (d < Sb) {
-      const int64_t pd = (int32_t)r[d][q];
-      if (d < 3) g0 = g0 * 128 + pd;
-      else if (d < 5) g1 = g1 * 128 + pd;
-      else g2 = g2 * 128 + pd;
-    }
-  }
-  double acc = i2d_small(g0) * pow2i(-7 * ((Sb < 3 ? Sb : 3) + 1));
-  if (Sb > 3) acc = fma(i2d_small(g1), pow2i(-7 * ((Sb < 5 ? Sb : 5) + 1)), acc);
-  if (Sb > 5) acc = fma(i2d_small(g2), pow2i(-7 * (Sb + 1)), acc);
+  for (int d = 1; d < S; ++d)
+    if (d < Sb) acc = fma(acc, 128.0, i32_to_f64(r[d][q]));
   return acc;
 }
 
@@ -1046,7 +1038,9 @@ __global__ void __launch_bounds__(kFusedThreads, 1) gemm_split_fused_kernel(cons
         // become zero and are never stored
         const bool rok = i < Mreal;
         ei = rok ? max(eA[i], -1100) : -1100;
-        const double rscale = (ei >= -1022 && ei <= 1023) ? pow2i(ei) : 0.0;
+        // the row scale carries the recombination's 2^(−7(sb+1))
+        const int eis = ei - 7 * (sb + 1);
+        const double rscale = (eis >= -1022 && eis <= 1023) ? pow2i(eis) : 0.0;
         // lane l holds the exponent and scale of the warp's column 32·half + l (shared by shuffles)
         const int64_t jl = it.n0 + 32 * half + lane;
         const bool cok = jl < b.n;
@@ -1077,13 +1071,15 @@ __global__ void __launch_bounds__(kFusedThreads, 1) gemm_split_fused_kernel(cons
 #pragma unroll
             for (int q = 0; q < 8; ++q) w[q] = recombine_value<S, 8>(r, q, sb);
           }
+          if (!slow) {
 #pragma unroll
-          for (int q = 0; q < 8; ++q) {
-            const int ejq = __shfl_sync(0xffffffffu, ej, 8 * g8 + q);
-            const double csq = __shfl_sync(0xffffffffu, cs, 8 * g8 + q);
-            w[q] = slow ? scale2(w[q], ei + ejq) : w[q] * rscale * csq;
-            vmax = fmax(vmax, fabs(w[q]));
+            for (int q = 0; q < 8; ++q) w[q] = w[q] * rscale * __shfl_sync(0xffffffffu, cs, 8 * g8 + q);
+          } else {
+#pragma unroll
+            for (int q = 0; q < 8; ++q) w[q] = scale2(w[q], eis + __shfl_sync(0xffffffffu, ej, 8 * g8 + q));
           }
+#pragma unroll
+          for (int q = 0; q < 8; ++q) vmax = fmax(vmax, fabs(w[q]));
           if (direct) {
             store_group<CPLX>(w, i, it.n0 + c0, b, g.C, g.alpha, g.beta, true);
           } else {
