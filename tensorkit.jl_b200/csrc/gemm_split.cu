@@ -472,21 +472,27 @@ __device__ unsigned long long tkb_tl[kTlCtas * kTlSlots];
 #define TL_ADD(k, v) ((void)0)
 #define TL_NOW() 0ull
 #endif
-// bounded wait on a phase parity: false once 2 s of wall time have passed
+// one test of a phase parity (the hardware may suspend the thread for a while before it answers)
+__device__ __forceinline__ bool mbar_try(uint32_t addr, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.b32 %0, 1, 0, p;\n\t}\n"
+      : "=r"(ok)
+      : "r"(addr), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// bounded wait on a phase parity: false once 2 s of wall time have passed. A phase that has
+// completed costs one test; the clock is read only after the first test fails, then every 64.
 __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity) {
   const uint32_t addr = smem_u32(bar);
+  if (mbar_try(addr, parity)) return true;
   const uint64_t t0 = globaltimer_ns();
-  while (true) {
-    uint32_t ok;
-    asm volatile(
-        "{\n\t.reg .pred p;\n\t"
-        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-        "selp.b32 %0, 1, 0, p;\n\t}\n"
-        : "=r"(ok)
-        : "r"(addr), "r"(parity)
-        : "memory");
-    if (ok) return true;
-    if (globaltimer_ns() - t0 > 2000000000ull) return false;
+  for (uint32_t n = 1;; ++n) {
+    if (mbar_try(addr, parity)) return true;
+    if ((n & 63u) == 0 && globaltimer_ns() - t0 > 2000000000ull) return false;
   }
 }
 __device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t bytes, uint64_t *bar) {
@@ -756,21 +762,15 @@ struct FusedArgs {
   int fixed;                // 1: the caller fixed the slice count (every block uses S, no check)
 };
 
-// bounded mbarrier wait that also gives up when the CTA aborts
+// bounded mbarrier wait that also gives up when the CTA aborts (a completed phase costs one test)
 __device__ __forceinline__ bool mbar_wait_abortable(uint64_t *bar, uint32_t parity, const volatile int *abort) {
   const uint32_t addr = smem_u32(bar);
+  if (mbar_try(addr, parity)) return true;
   const uint64_t t0 = globaltimer_ns();
-  while (true) {
-    uint32_t ok;
-    asm volatile(
-        "{\n\t.reg .pred p;\n\t"
-        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-        "selp.b32 %0, 1, 0, p;\n\t}\n"
-        : "=r"(ok)
-        : "r"(addr), "r"(parity)
-        : "memory");
-    if (ok) return true;
-    if (*abort || globaltimer_ns() - t0 > 2000000000ull) return false;
+  for (uint32_t n = 1;; ++n) {
+    if (mbar_try(addr, parity)) return true;
+    if (*abort) return false;
+    if ((n & 63u) == 0 && globaltimer_ns() - t0 > 2000000000ull) return false;
   }
 }
 __device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
@@ -901,10 +901,7 @@ __global__ void __launch_bounds__(kFusedThreads, 1) gemm_split_fused_kernel(cons
         for (int kt = it.kb; kt < it.ke; ++kt, ++gs) {
           const int st = gs % NSTAGE, n = gs / NSTAGE;
           if (n > 0) {
-            [[maybe_unused]] const unsigned long long te = TL_NOW();
-            const bool waited = mbar_wait_abortable(&empty[st], (n - 1) & 1, abort);
-            TL_ADD(26, TL_NOW() - te);
-            if (!waited) {
+            if (!mbar_wait_abortable(&empty[st], (n - 1) & 1, abort)) {
               atomicExch(g.err, 1);
               *abort = 1;
               ok = false;
@@ -944,14 +941,15 @@ __global__ void __launch_bounds__(kFusedThreads, 1) gemm_split_fused_kernel(cons
         const uint32_t ring0 = smem_u32(smem);
         for (int kt = it.kb; kt < it.ke; ++kt, ++gs) {
           const int st = gs % NSTAGE;
-          [[maybe_unused]] const unsigned long long tf = TL_NOW();
-          const bool landed = mbar_wait_abortable(&full[st], (gs / NSTAGE) & 1, abort);
-          TL_ADD(25, TL_NOW() - tf);
-          if (!landed) {
+          if (!mbar_wait_abortable(&full[st], (gs / NSTAGE) & 1, abort)) {
             atomicExch(g.err, 1);
             *abort = 1;
             ok = false;
             break;
+          }
+          if (li == 0 && kt == it.kb) {
+            TL_STAMP(2);
+            TL_ADD(15, it.ke - it.kb);
           }
           tc_fence_after();
           const uint32_t a0 = ring0 + st * STAGE, b0 = a0 + A_BYTES;
