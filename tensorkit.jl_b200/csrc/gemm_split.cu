@@ -39,6 +39,8 @@
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
+#include <map>
+#include <mutex>
 #include <numeric>
 
 #include "tkb_internal.h"
@@ -49,10 +51,11 @@ constexpr int PANEL_A = 128, PANEL_B = 64;   // rows per panel
 constexpr int KSTAGE = 32;                   // bytes of K per stage (one tensor-core K step)
 constexpr int kSmemMax = 232448;             // dynamic shared memory per CTA (227 KiB)
 constexpr int kSmemTail = 2048;              // barriers and small tables after the ring
+constexpr int kXchgBytes = 2 * 128 * 32 * 8;  // split tiles: this CTA's column half and the peer's
 // depth of the shared-memory ring: as many stages of S slices of A and B as fit, at most 8
 __host__ __device__ constexpr int ring_stages(int S) {
-  return (kSmemMax - kSmemTail) / (S * (PANEL_A + PANEL_B) * KSTAGE) < 8
-             ? (kSmemMax - kSmemTail) / (S * (PANEL_A + PANEL_B) * KSTAGE)
+  return (kSmemMax - kSmemTail - kXchgBytes) / (S * (PANEL_A + PANEL_B) * KSTAGE) < 8
+             ? (kSmemMax - kSmemTail - kXchgBytes) / (S * (PANEL_A + PANEL_B) * KSTAGE)
              : 8;
 }
 constexpr int SMAX = 7;
@@ -637,12 +640,15 @@ __device__ __forceinline__ typename SrcVal<CPLX>::T opB_at(const GBlock &b, cons
 
 // FP64 fallback: the eight epilogue warps compute one whole output tile with DMMA
 // (mma.sync.m8n8k4.f64) from the FP64 operands over the full K range, and store α·C + β·C_old.
+// (The four warps of one column half, called alone with n0 moved by 32·half and warp − 4·half,
+// compute that half.)
 // Real: tile rows m0 .. m0+127, warp (w mod 4, w / 4) takes 32 rows × 32 columns. Complex: the
 // tile's real row pairs are complex rows m0/2 .. m0/2+63; a warp takes 16 complex rows × 32
 // columns, four real DMMA per complex product.
 template <bool CPLX>
 __device__ __noinline__ void fp64_tile(const GBlock &b, int64_t m0, int64_t n0, const void *A, const void *B,
                                        double *C, CDbl alpha, CDbl beta, bool bz, int warp, int lane) {
+  if (n0 >= b.n) return;
   const int g8 = lane >> 2, t4 = lane & 3;
   if constexpr (!CPLX) {
     const int64_t r0 = m0 + 32 * (warp & 3), c0 = n0 + 32 * (warp >> 2);
@@ -776,6 +782,53 @@ __device__ __forceinline__ bool mbar_wait_abortable(uint64_t *bar, uint32_t pari
 __device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
   asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(smem_u32(bar)) : "memory");
 }
+// ---- the two CTAs of a cluster (split tiles exchange column halves) ---------------------------
+__device__ __forceinline__ uint32_t cluster_rank() {
+  uint32_t r;
+  asm volatile("mov.u32 %0, %%cluster_ctarank;\n" : "=r"(r));
+  return r;
+}
+// the shared::cluster address of this CTA's shared-memory address in CTA `rank` of the cluster
+__device__ __forceinline__ uint32_t peer_addr(uint32_t saddr, uint32_t rank) {
+  uint32_t r;
+  asm volatile("mapa.shared::cluster.u32 %0, %1, %2;\n" : "=r"(r) : "r"(saddr), "r"(rank));
+  return r;
+}
+__device__ __forceinline__ void st_peer_f64(uint32_t addr, double v) {
+  asm volatile("st.shared::cluster.f64 [%0], %1;\n" ::"r"(addr), "d"(v) : "memory");
+}
+// arrive on an mbarrier of the peer CTA, releasing this thread's earlier writes at cluster scope
+__device__ __forceinline__ void mbar_arrive_peer(uint32_t addr) {
+  asm volatile("mbarrier.arrive.release.cluster.shared::cluster.b64 _, [%0];\n" ::"r"(addr) : "memory");
+}
+__device__ __forceinline__ void fence_cluster() { asm volatile("fence.acq_rel.cluster;\n" ::: "memory"); }
+// every thread of both CTAs (release / acquire at cluster scope)
+__device__ __forceinline__ void cluster_sync_all() {
+  asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;\n" ::: "memory");
+}
+// bounded wait on a phase parity with acquire at cluster scope (arrivals of the peer CTA);
+// false once 2 s have passed or the CTA aborts
+__device__ __forceinline__ bool mbar_wait_cluster(uint64_t *bar, uint32_t parity, const volatile int *abort) {
+  const uint32_t addr = smem_u32(bar);
+  auto test = [&]() {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.acquire.cluster.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.b32 %0, 1, 0, p;\n\t}\n"
+        : "=r"(ok)
+        : "r"(addr), "r"(parity)
+        : "memory");
+    return ok != 0;
+  };
+  if (test()) return true;
+  const uint64_t t0 = globaltimer_ns();
+  for (uint32_t n = 1;; ++n) {
+    if (test()) return true;
+    if (*abort) return false;
+    if ((n & 63u) == 0 && globaltimer_ns() - t0 > 2000000000ull) return false;
+  }
+}
 __device__ __forceinline__ void epi_sync() {
   asm volatile("bar.sync %0, %1;\n" ::"n"(kEpiBarrier), "n"(kEpiWarps * 32) : "memory");
 }
@@ -839,20 +892,28 @@ __global__ void __launch_bounds__(kFusedThreads, 1) gemm_split_fused_kernel(cons
   constexpr uint32_t STAGE = A_BYTES + B_BYTES;
   constexpr int NSTAGE = ring_stages(S);
   extern __shared__ __align__(1024) unsigned char smem[];
-  uint64_t *full = reinterpret_cast<uint64_t *>(smem + NSTAGE * STAGE);
+  // split tiles: this CTA's column half of its own piece (xo) and the peer's piece for it (xr),
+  // [column][row] of 32 × 128
+  double *xo = reinterpret_cast<double *>(smem + NSTAGE * STAGE);
+  double *xr = xo + 32 * 128;
+  uint64_t *full = reinterpret_cast<uint64_t *>(smem + NSTAGE * STAGE + kXchgBytes);
   uint64_t *empty = full + NSTAGE;
   uint64_t *acc_full = full + 2 * NSTAGE;
   uint64_t *acc_empty = acc_full + 1;
   uint64_t *drain = acc_full + 2;
   uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(acc_full + 3);
-  int *claim = reinterpret_cast<int *>(acc_full + 4);  // [2]: split-K arrival ticket
-  volatile int *abort = claim + 3;
+  volatile int *abort = reinterpret_cast<int *>(acc_full + 4);
+  uint64_t *xfull = acc_full + 5;   // xr holds the peer's half (4 arrivals of the peer's warps)
+  uint64_t *xempty = acc_full + 6;  // the peer has read this CTA's half out of its xr (4 arrivals)
   // tile check: per epilogue warp, largest |C|, row exponent and column exponent (two buffers)
-  double *gmax = reinterpret_cast<double *>(acc_full + 6);    // [2][kEpiWarps]
+  double *gmax = reinterpret_cast<double *>(acc_full + 8);    // [2][kEpiWarps]
   int *gexp = reinterpret_cast<int *>(gmax + 2 * kEpiWarps);        // [2][kEpiWarps][2]
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const FusedArgs &g = args;
-  int *arrive = g.cnt + 4;
+  // the cluster of two CTAs takes the item pairs cl, cl + ncl, …; rank r the pair's item r
+  const int rank = (int)cluster_rank(), peer = rank ^ 1;
+  const int cl = (int)blockIdx.x >> 1, ncl = (int)gridDim.x >> 1;
+  auto item_of = [&](int k) { return 2 * (cl + k * ncl) + rank; };
   if (tid == 0) TL_STAMP(0);
 
   if (tid == 0) {
@@ -864,6 +925,8 @@ __global__ void __launch_bounds__(kFusedThreads, 1) gemm_split_fused_kernel(cons
     mbar_init(acc_full, 1);
     mbar_init(acc_empty, kEpiWarps);
     mbar_init(drain, 1);
+    mbar_init(xfull, kEpiWarps / 2);
+    mbar_init(xempty, kEpiWarps / 2);
     *abort = 0;
     asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
   }
@@ -874,24 +937,26 @@ __global__ void __launch_bounds__(kFusedThreads, 1) gemm_split_fused_kernel(cons
   }
   tc_fence_before();
   __syncthreads();
+  cluster_sync_all();  // the peer's barriers are initialised before any arrival on them
   tc_fence_after();
   const uint32_t tmem = *tmem_slot;
   pdl_wait();  // the slicing launch has finished; C comes from earlier kernels of the stream
   if (tid == 0) TL_STAMP(1);
 
   // ---- products ------------------------------------------------------------------
-  const int G = gridDim.x;
   // a block's slice count (0: the block runs in FP64) from the statistics of the slicing launch
-  auto slices_of = [&](int block, int kpad) -> int { return g.fixed ? S : choose_slices<S>(g.bst, block, kpad); };
+  auto slices_of = [&](const GBlock &b, int block) -> int {
+    return b.fp64only ? 0 : g.fixed ? S : choose_slices<S>(g.bst, block, b.kpad);
+  };
   if (warp == kProducerWarp) {
     if (lane == 0) {
       int issued = 0, landed = 0;  // stages issued / known to have landed (for the final drain)
       int gs = 0;                  // ring stage counter over all items of this CTA
-      for (int ii = blockIdx.x; ii < g.nitems && !*abort; ii += G) {
+      for (int k = 0, ii = item_of(0); ii < g.nitems && !*abort; ii = item_of(++k)) {
         const SplitTile it = g.items[ii];
         if (it.kind != 0) continue;
         const GBlock b = g.blocks[it.block];
-        const int sb = slices_of(it.block, b.kpad);
+        const int sb = slices_of(b, it.block);
         if (issued == 0) TL_STAMP(7);
         if (sb == 0) continue;  // the block runs in FP64
         fence_proxy_async_global();
@@ -927,10 +992,10 @@ __global__ void __launch_bounds__(kFusedThreads, 1) gemm_split_fused_kernel(cons
     if (lane == 0) {
       int gs = 0, li = 0;
       bool ok = true;
-      for (int ii = blockIdx.x; ii < g.nitems && ok && !*abort; ii += G) {
+      for (int k = 0, ii = item_of(0); ii < g.nitems && ok && !*abort; ii = item_of(++k)) {
         const SplitTile it = g.items[ii];
         if (it.kind != 0) continue;
-        const int sb = slices_of(it.block, g.blocks[it.block].kpad);
+        const int sb = slices_of(g.blocks[it.block], it.block);
         if (sb == 0) continue;
         if (li > 0 && !mbar_wait_abortable(acc_empty, (li - 1) & 1, abort)) {
           atomicExch(g.err, 2);
@@ -984,20 +1049,28 @@ __global__ void __launch_bounds__(kFusedThreads, 1) gemm_split_fused_kernel(cons
     }
     __syncwarp();
   } else {
-    // epilogue warps: warp w owns TMEM lanes 32(w mod 4) .. +31 (its rows) and the column chunks
-    // 2·half, 2·half + 1 of 16 columns, half = w / 4
+    // epilogue warps: warp w owns TMEM lanes 32(w mod 4) .. +31 (its rows) and the 32 columns
+    // 32·half .. +31, half = w / 4. In a split tile (two K pieces on the two CTAs of the cluster)
+    // CTA r keeps column half r: its warps of half r put their values into xo, the warps of the
+    // other half send theirs into the peer's xr; the warps of half r then add xo and xr, check and
+    // store that half.
     const int quarter = warp & 3, half = warp >> 2;
     const int row = 32 * quarter + lane;
+    const bool keeper = half == rank;
     constexpr bool bz = BZ;
-    int li = 0, gi = 0;
-    for (int ii = blockIdx.x; ii < g.nitems; ii += G) {
+    const uint32_t xr_peer = peer_addr(smem_u32(xr), (uint32_t)peer);
+    const uint32_t xempty_peer = peer_addr(smem_u32(xempty), (uint32_t)peer);
+    const uint32_t xfull_peer = peer_addr(smem_u32(xfull), (uint32_t)peer);
+    int li = 0, gi = 0, ns = 0;  // items with products, checked tiles, exchanged split tiles
+    for (int k = 0, ii = item_of(0); ii < g.nitems; ii = item_of(++k)) {
       const SplitTile it = g.items[ii];
+      if (it.kind == 2) continue;  // the empty half of a pair
       const GBlock b = g.blocks[it.block];
       const int64_t Mreal = CPLX ? 2 * b.m : b.m;
       const int64_t i = it.m0 + row;
       const bool prod = it.kind == 0;
       bool stop = *abort != 0;
-      const int sb = prod ? slices_of(it.block, b.kpad) : 0;
+      const int sb = prod ? slices_of(b, it.block) : 0;
       const bool mma = prod && sb > 0;  // the tile's products ran on the tensor cores
       [[maybe_unused]] const unsigned long long ta = TL_NOW();
       if (mma && !stop) stop = !mbar_wait_abortable(acc_full, li & 1, abort);
@@ -1015,17 +1088,16 @@ __global__ void __launch_bounds__(kFusedThreads, 1) gemm_split_fused_kernel(cons
         break;
       }
       if (prod && !mma) {
-        // FP64 block: one piece (the first) computes the whole tile over the full K range
+        // FP64 block: the first piece computes the whole tile over the full K range
         if (it.sid == 0) fp64_tile<CPLX>(b, it.m0, it.n0, g.A, g.B, g.C, g.alpha, g.beta, bz, warp, lane);
         continue;
       }
       const bool split = it.nsplit > 1;
       // direct: β = 0 and one piece, so the values go to C as they are recombined (a tile the
-      // check sends to FP64 is overwritten). Otherwise they go to a scratch tile ([col][row]) first:
-      // this piece's partial (split), or the CTA's hold tile (β ≠ 0: C keeps its old values until
-      // the tile check has passed).
+      // check sends to FP64 is overwritten). β ≠ 0, one piece: they wait in the CTA's hold tile
+      // ([col][row], global) until the check has passed.
       const bool direct = BZ && !split;
-      double *scr = g.part + (int64_t)(split ? it.pbase + it.sid : g.hold0 + (int)blockIdx.x) * (64 * 128);
+      double *scr = g.part + (int64_t)(g.hold0 + (int)blockIdx.x) * (64 * 128);
       double vmax = 0.0;    // largest |C| of the thread's values
       int ei = 0, ejm = 0;  // the thread's row exponent, the largest column exponent of its columns
       if (mma) {
@@ -1047,6 +1119,8 @@ __global__ void __launch_bounds__(kFusedThreads, 1) gemm_split_fused_kernel(cons
         ejm = ej;
         // the exact (ldexp) scaling only where a real row's or column's 2^e is not a normal double
         const bool slow = __any_sync(0xffffffffu, (rok && rscale == 0.0) || (cok && cs == 0.0));
+        // a sending warp may overwrite the peer's xr once the peer has read the previous split tile
+        if (split && !keeper && ns > 0 && !mbar_wait_cluster(xempty, (ns - 1) & 1, abort)) stop = true;
         // the warp's 32 columns, 8 at a time (a runtime loop: the code stays small); after the
         // last group's loads the accumulators go back to the MMA warp
 #pragma unroll 1
@@ -1080,9 +1154,15 @@ __global__ void __launch_bounds__(kFusedThreads, 1) gemm_split_fused_kernel(cons
           for (int q = 0; q < 8; ++q) vmax = fmax(vmax, fabs(w[q]));
           if (direct) {
             store_group<CPLX>(w, i, it.n0 + c0, b, g.C, g.alpha, g.beta, true);
-          } else {
+          } else if (!split) {
 #pragma unroll
             for (int q = 0; q < 8; ++q) __stcg(&scr[(c0 + q) * 128 + row], w[q]);
+          } else if (keeper) {
+#pragma unroll
+            for (int q = 0; q < 8; ++q) xo[(8 * g8 + q) * 128 + row] = w[q];
+          } else if (!stop) {
+#pragma unroll
+            for (int q = 0; q < 8; ++q) st_peer_f64(xr_peer + (uint32_t)(((8 * g8 + q) * 128 + row) * 8), w[q]);
           }
           if (tid == 0 && li == 0 && g8 == 0) TL_STAMP(13);
         }
@@ -1092,45 +1172,7 @@ __global__ void __launch_bounds__(kFusedThreads, 1) gemm_split_fused_kernel(cons
         }
         ++li;
       }
-      [[maybe_unused]] const unsigned long long ts = TL_NOW();
-      bool final_piece = true;
-      if (split) {
-        if (tid == 0) TL_ADD(19, 1);
-        // count this piece (its partial is stored); the last piece adds all partials in piece
-        // order into its own partial tile
-        __threadfence();
-        epi_sync();
-        if (tid == 0) claim[2] = atomicAdd(&arrive[it.slot], 1);
-        epi_sync();
-        final_piece = claim[2] == it.nsplit - 1;
-        epi_sync();  // the ticket slot is rewritten by the next item
-        if (final_piece) {
-          __threadfence();
-          // the thread's 32 values of every piece are loaded together (one latency per piece)
-          double v[32];
-#pragma unroll
-          for (int q = 0; q < 32; ++q) v[q] = 0.0;
-#pragma unroll 1
-          for (int sp = 0; sp < it.nsplit; ++sp) {
-            const double *src = g.part + (int64_t)(it.pbase + sp) * (64 * 128) + (32 * half) * 128 + row;
-#pragma unroll
-            for (int q = 0; q < 32; ++q) v[q] += __ldcg(&src[q * 128]);
-          }
-          vmax = 0.0;
-#pragma unroll
-          for (int q = 0; q < 32; ++q) {
-            vmax = fmax(vmax, fabs(v[q]));
-            __stcg(&scr[(32 * half + q) * 128 + row], v[q]);
-          }
-          if (tid == 0) {
-            arrive[it.slot] = 0;  // every piece has arrived: free for the next launch
-            TL_ADD(20, 1);
-          }
-        }
-      }
-      if (tid == 0) TL_ADD(23, TL_NOW() - ts);
-      if (!final_piece) continue;  // uniform: every epilogue thread read the same ticket
-      if (!mma) {                  // β-scale only (k = 0)
+      if (!mma) {  // β-scale only (k = 0)
 #pragma unroll 1
         for (int g8 = 0; g8 < 4; ++g8) {
           const double w[8] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
@@ -1138,7 +1180,43 @@ __global__ void __launch_bounds__(kFusedThreads, 1) gemm_split_fused_kernel(cons
         }
         continue;
       }
-      // tile check: largest |C| and exponents of the tile against the error estimate
+      [[maybe_unused]] const unsigned long long ts = TL_NOW();
+      if (split) {
+        // sending warps: their values are in the peer's xr; keeping warps: wait for the peer's
+        // half, add it to their own (two terms: the order does not matter), then free xr
+        if (!keeper) {
+          fence_cluster();
+          __syncwarp();
+          if (lane == 0) mbar_arrive_peer(xfull_peer);
+          vmax = 0.0;
+          ei = -1100;
+          ejm = -1100;
+        } else {
+          if (!mbar_wait_cluster(xfull, ns & 1, abort)) stop = true;
+          vmax = 0.0;
+#pragma unroll 4
+          for (int q = 0; q < 32; ++q) {
+            const double v = xo[q * 128 + row] + xr[q * 128 + row];
+            xo[q * 128 + row] = v;
+            vmax = fmax(vmax, fabs(v));
+          }
+          fence_cluster();
+          __syncwarp();
+          if (lane == 0) mbar_arrive_peer(xempty_peer);
+        }
+        ++ns;
+        if (epi_any(stop)) {
+          if (tid == 0) {
+            atomicExch(g.err, 2);
+            *abort = 1;
+          }
+          break;
+        }
+        if (tid == 0) TL_ADD(19, 1);
+      }
+      if (tid == 0) TL_ADD(23, TL_NOW() - ts);
+      // tile check (a split tile: this CTA's column half): largest |C| and exponents against
+      // the error estimate
       [[maybe_unused]] const unsigned long long tg = TL_NOW();
       double vm = vmax;
 #pragma unroll
@@ -1165,11 +1243,25 @@ __global__ void __launch_bounds__(kFusedThreads, 1) gemm_split_fused_kernel(cons
       if (!g.fixed && est > kSliceTol * tmax) {  // uniform over the epilogue warps
         if (tid == 0) atomicAdd(&g.cnt[2], 1);
         if (direct) epi_sync();  // every approximate value of the tile is stored before the overwrite
-        fp64_tile<CPLX>(b, it.m0, it.n0, g.A, g.B, g.C, g.alpha, g.beta, bz, warp, lane);
+        if (!split) {
+          fp64_tile<CPLX>(b, it.m0, it.n0, g.A, g.B, g.C, g.alpha, g.beta, bz, warp, lane);
+        } else if (keeper) {  // this CTA's column half
+          fp64_tile<CPLX>(b, it.m0, it.n0 + 32 * rank, g.A, g.B, g.C, g.alpha, g.beta, bz, warp - 4 * rank, lane);
+        }
         continue;
       }
-      if (!direct) {
-        // the checked values from the scratch tile (written by this thread) to C
+      if (split) {
+        if (keeper) {
+#pragma unroll 1
+          for (int g8 = 0; g8 < 4; ++g8) {
+            double w[8];
+#pragma unroll
+            for (int q = 0; q < 8; ++q) w[q] = xo[(8 * g8 + q) * 128 + row];
+            store_group<CPLX>(w, i, it.n0 + 32 * half + 8 * g8, b, g.C, g.alpha, g.beta, bz);
+          }
+        }
+      } else if (!direct) {
+        // the checked values from the hold tile (written by this thread) to C
 #pragma unroll 1
         for (int g8 = 0; g8 < 4; ++g8) {
           const int c0 = 32 * half + 8 * g8;
@@ -1187,6 +1279,7 @@ __global__ void __launch_bounds__(kFusedThreads, 1) gemm_split_fused_kernel(cons
   // ---- teardown ----------------------------------------------------------------------------
   tc_fence_before();
   __syncthreads();
+  cluster_sync_all();  // no CTA leaves while its peer may still reach its shared memory
   if (tid == 0) TL_STAMP(17);
   if (warp == kMmaWarp) {
     tc_fence_after();
@@ -1247,7 +1340,9 @@ __global__ void __launch_bounds__(kSliceThreads, 2) gemm_split_slice_kernel(cons
   if (lane == 0) TL_MAX(29, TL_NOW());
 }
 
-size_t tc_smem_bytes(int S) { return ring_stages(S) * (size_t)S * (PANEL_A + PANEL_B) * KSTAGE + kSmemTail; }
+size_t tc_smem_bytes(int S) {
+  return ring_stages(S) * (size_t)S * (PANEL_A + PANEL_B) * KSTAGE + kXchgBytes + kSmemTail;
+}
 
 template <int S>
 int launch_split(tkb_ctx *ctx, const tkb_plan *p, void *C, const void *A, const void *B, CDbl a, CDbl b) {
@@ -1284,7 +1379,38 @@ int launch_split(tkb_ctx *ctx, const tkb_plan *p, void *C, const void *A, const 
     TKB_CUDA_TRY(ctx, launch_pdl(ks, dim3((unsigned)grid), dim3(kSliceThreads), 0, ctx->stream, fa));
     ctx->launches++;
   }
-  TKB_CUDA_TRY(ctx, launch_pdl(k, dim3((unsigned)ctx->num_sms), dim3(kFusedThreads), smem, ctx->stream, fa));
+  // two-CTA clusters, as many as can be resident at once (the persistent loop takes the rest)
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3((unsigned)(ctx->num_sms & ~1));
+  cfg.blockDim = dim3(kFusedThreads);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = ctx->stream;
+  cudaLaunchAttribute attr[2];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  attr[1].id = cudaLaunchAttributeClusterDimension;
+  attr[1].val.clusterDim.x = 2;
+  attr[1].val.clusterDim.y = 1;
+  attr[1].val.clusterDim.z = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 2;
+  static std::mutex mu;
+  static std::map<std::pair<const void *, int>, int> active;  // (kernel, device) → resident clusters
+  int ncl = 0;
+  {
+    std::lock_guard<std::mutex> lk(mu);
+    auto key = std::make_pair((const void *)k, ctx->device);
+    auto f = active.find(key);
+    if (f != active.end()) {
+      ncl = f->second;
+    } else {
+      TKB_CUDA_TRY(ctx, cudaOccupancyMaxActiveClusters(&ncl, k, &cfg));
+      active[key] = ncl;
+    }
+  }
+  if (ncl < 1) return tkb_set_error(ctx, TKB_ERR_CUDA, "split GEMM: no two-CTA cluster fits an SM pair");
+  cfg.gridDim = dim3((unsigned)(2 * std::min(ncl, ctx->num_sms / 2)));
+  TKB_CUDA_TRY(ctx, cudaLaunchKernelEx(&cfg, k, fa));
   ctx->launches++;
   TKB_CUDA_TRY(ctx, cudaGetLastError());
   return TKB_OK;
@@ -1407,50 +1533,49 @@ int tkb_gemm_split_prepare(tkb_ctx *ctx, tkb_plan *p) {
   std::stable_sort(tiles.begin(), tiles.end(), [&](const GTile &x, const GTile &y) {
     return p->hblocks[x.block].kpad > p->hblocks[y.block].kpad;
   });
-  // products items of the persistent kernel (one CTA per SM). With fewer tiles than SMs the K
-  // loops are cut into pieces of about `target` stages, the smallest target (≥ min_piece_steps) whose
-  // item count still fits one round of the CTAs, so the longest item is as short as possible.
+  // products items in pairs, one pair per two-CTA cluster of the persistent kernel: a split tile
+  // (its two K halves, one per CTA) or two unsplit tiles (the second may be empty). As many of the
+  // longest tiles are split as keep the pairs within one cluster round (num_sms / 2 pairs), when
+  // the decomposition allows it (max_pieces ≥ 2, halves of at least min_piece_steps stages). A tile
+  // whose K needs more than one exact piece (int32 accumulators stay exact over (2^31 − 1)/(S·127²)
+  // K positions) is split in any case; a block whose K needs more than two runs in FP64.
   std::vector<SplitTile> kt;
   int nslots = 0, npart = 0;
   {
-    const int64_t nt = (int64_t)tiles.size();
-    const int64_t nsm = ctx->num_sms;
-    int64_t total = 0, maxnk = 1;
-    for (const GTile &t : tiles)
-      if (t.kind == 0) {
-        total += p->hblocks[t.block].kpad / KSTAGE;
-        maxnk = std::max<int64_t>(maxnk, p->hblocks[t.block].kpad / KSTAGE);
-      }
-    // int32 accumulators stay exact over at most (2^31 − 1)/(S·127²) K positions per item
     const int64_t maxst = std::max<int64_t>(1, (int64_t)2147483647 / ((int64_t)S * 127 * 127) / KSTAGE);
-    auto pieces = [&](int64_t nk, int64_t target) {
-      return (int)std::max<int64_t>(std::min<int64_t>(p->max_pieces, (nk + target - 1) / target),
-                                    (nk + maxst - 1) / maxst);
+    const int64_t ncl = std::max<int64_t>(1, ctx->num_sms / 2);
+    for (GBlock &b : p->hblocks)
+      if (b.kpad / KSTAGE > 2 * maxst) b.fp64only = 1;
+    const int64_t nt = (int64_t)tiles.size();
+    int64_t budget = p->max_pieces >= 2 ? std::max<int64_t>(0, 2 * ncl - nt) : 0;  // tiles to split
+    struct Pair {
+      SplitTile a, b;
+      int64_t cost;
     };
-    int64_t target = maxnk;  // no split
-    if (nt < nsm) {
-      target = std::max<int64_t>(p->min_piece_steps, (total + nsm - 1) / nsm);
-      for (; target < maxnk; ++target) {
-        int64_t cnt = 0;
-        for (const GTile &t : tiles) cnt += t.kind == 0 ? pieces(p->hblocks[t.block].kpad / KSTAGE, target) : 1;
-        if (cnt <= nsm) break;
-      }
-    }
-    for (const GTile &t : tiles) {
-      const int nk = p->hblocks[t.block].kpad / KSTAGE;
-      const int ks = t.kind == 0 ? pieces(nk, target) : 1;
-      if (ks == 1) {
-        kt.push_back({t.block, t.m0, t.n0, t.kind, 0, t.kind == 0 ? nk : 0, -1, 1, 0, 0});
+    std::vector<Pair> pairs;
+    std::vector<SplitTile> singles;
+    const SplitTile none{0, 0, 0, 2, 0, 0, -1, 1, 0, 0};
+    for (const GTile &t : tiles) {  // longest K first
+      const int nk = t.kind == 0 ? p->hblocks[t.block].kpad / KSTAGE : 0;
+      const bool must = t.kind == 0 && nk > maxst && !p->hblocks[t.block].fp64only;
+      const bool may = t.kind == 0 && budget > 0 && nk >= 2 * p->min_piece_steps;
+      if (must || may) {
+        if (!must) --budget;
+        pairs.push_back({{t.block, t.m0, t.n0, 0, 0, nk / 2, -1, 2, 0, 0},
+                         {t.block, t.m0, t.n0, 0, nk / 2, nk, -1, 2, 1, 0}, (int64_t)(nk - nk / 2)});
       } else {
-        const int slot = nslots++;
-        for (int s = 0; s < ks; ++s)
-          kt.push_back({t.block, t.m0, t.n0, t.kind, s * nk / ks, (s + 1) * nk / ks, slot, ks, s, npart});
-        npart += ks;
+        singles.push_back({t.block, t.m0, t.n0, t.kind, 0, nk, -1, 1, 0, 0});
       }
     }
-    std::stable_sort(kt.begin(), kt.end(), [](const SplitTile &x, const SplitTile &y) {
-      return (x.ke - x.kb) > (y.ke - y.kb);
-    });
+    std::stable_sort(singles.begin(), singles.end(),
+                     [](const SplitTile &x, const SplitTile &y) { return (x.ke - x.kb) > (y.ke - y.kb); });
+    for (size_t q = 0; q < singles.size(); q += 2)
+      pairs.push_back({singles[q], q + 1 < singles.size() ? singles[q + 1] : none, (int64_t)(singles[q].ke - singles[q].kb)});
+    std::stable_sort(pairs.begin(), pairs.end(), [](const Pair &x, const Pair &y) { return x.cost > y.cost; });
+    for (const Pair &pr : pairs) {
+      kt.push_back(pr.a);
+      kt.push_back(pr.b);
+    }
   }
   p->ws_bytes = off;
   p->nstiles = (int64_t)tiles.size();
@@ -1465,8 +1590,7 @@ int tkb_gemm_split_prepare(tkb_ctx *ctx, tkb_plan *p) {
     e = cudaMalloc(&p->kstiles, kt.size() * sizeof(SplitTile));
     if (e == cudaSuccess) e = cudaMemcpy(p->kstiles, kt.data(), kt.size() * sizeof(SplitTile), cudaMemcpyHostToDevice);
   }
-  // the partial tiles of the split items, then one hold tile per CTA (β ≠ 0: the recombined
-  // values wait there for the tile check)
+  // one hold tile per CTA (β ≠ 0, one piece: the recombined values wait there for the tile check)
   p->part_hold0 = npart;
   if (e == cudaSuccess && !kt.empty())
     e = cudaMalloc((void **)&p->part, (size_t)(npart + ctx->num_sms) * 64 * 128 * sizeof(double));

@@ -170,6 +170,7 @@ struct GBlock {
   int64_t wsA, wsB, wsEA, wsEB;
   int32_t mpad, npad, kpad;   // padded extents (tile multiples) of the sliced operands
   int32_t skinny;             // 1: n, k ≤ 16 — memory-bound row kernel in every precision
+  int32_t fp64only;           // split precision: K too long for two exact int32 pieces — FP64 tiles
 };
 
 constexpr int kSkinnyMax = 16;        // n and k bound of the skinny (row-per-thread) path

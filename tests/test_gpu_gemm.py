@@ -80,9 +80,10 @@ def test_split_error_decreases_with_slices(slices):
 
 @pytest.mark.parametrize("cplx", [False, True])
 def test_split_k_reductions(cplx):
-    """Few output tiles with long K: the K loops are split into pieces; the piece that arrives
-    last on a tile's counter adds the partial tiles in piece order and applies α and β. Run
-    twice through the cached plan (the counters clear themselves between launches)."""
+    """Few output tiles with long K: a tile's K loop is split into two halves that run on the two
+    CTAs of a cluster; each CTA adds the peer's half of the columns it keeps (through the peer's
+    shared memory) and applies α and β to that half. Run twice through the cached plan (the
+    exchange barriers and counters are fresh or cleared between launches)."""
     A, B = _mats(cplx, mult=8)
     ref = O.mul(A, B)
     C0 = O.randn(ref.W, 4, cplx)
@@ -96,8 +97,8 @@ def test_split_k_reductions(cplx):
 
 def test_split_long_k_multiwave():
     """K beyond the exact int32 range of one products item (≈ 19K positions at 7 slices) forces
-    at least two pieces per tile, and more pieces than CTAs: the last piece to arrive adds the
-    partials, no piece waits for another."""
+    two pieces per tile (the two CTAs of a cluster), and more tile pairs than clusters: the
+    persistent clusters take several pairs in turn."""
     Vm = O.Space({O.U1(0): 1024})
     Vk = O.Space({O.U1(0): 20000})
     Vn = O.Space({O.U1(0): 640})
