@@ -940,6 +940,13 @@ __global__ void __launch_bounds__(kFusedThreads, 1) gemm_split_fused_kernel(cons
   cluster_sync_all();  // the peer's barriers are initialised before any arrival on them
   tc_fence_after();
   const uint32_t tmem = *tmem_slot;
+  // the item table and block descriptors are plan constants: the first item and its block are
+  // brought into L1 while the slicing launch finishes
+  if (lane == 0 && item_of(0) < g.nitems) {
+    const SplitTile it0 = g.items[item_of(0)];
+    const char *pb = reinterpret_cast<const char *>(g.blocks + it0.block);
+    for (int o = 0; o < (int)sizeof(GBlock); o += 64) asm volatile("prefetch.L1 [%0];\n" ::"l"(pb + o));
+  }
   pdl_wait();  // the slicing launch has finished; C comes from earlier kernels of the stream
   if (tid == 0) TL_STAMP(1);
 
@@ -1072,6 +1079,14 @@ __global__ void __launch_bounds__(kFusedThreads, 1) gemm_split_fused_kernel(cons
       bool stop = *abort != 0;
       const int sb = prod ? slices_of(b, it.block) : 0;
       const bool mma = prod && sb > 0;  // the tile's products ran on the tensor cores
+      // the row exponent and the exponent of this lane's column, read before the products finish
+      const int32_t *eA = reinterpret_cast<const int32_t *>(g.ws + b.wsEA);
+      const int32_t *eB = reinterpret_cast<const int32_t *>(g.ws + b.wsEB);
+      const bool rok = i < Mreal;
+      const int64_t jl = it.n0 + 32 * half + lane;
+      const bool cok = jl < b.n;
+      const int eA_i = mma && rok ? eA[i] : -1100;
+      const int eB_j = mma && cok ? eB[jl] : -1100;
       [[maybe_unused]] const unsigned long long ta = TL_NOW();
       if (mma && !stop) stop = !mbar_wait_abortable(acc_full, li & 1, abort);
       if (tid == 0) {
@@ -1102,19 +1117,14 @@ __global__ void __launch_bounds__(kFusedThreads, 1) gemm_split_fused_kernel(cons
       int ei = 0, ejm = 0;  // the thread's row exponent, the largest column exponent of its columns
       if (mma) {
         tc_fence_after();
-        const int32_t *eA = reinterpret_cast<const int32_t *>(g.ws + b.wsEA);
-        const int32_t *eB = reinterpret_cast<const int32_t *>(g.ws + b.wsEB);
         // rows past the block (and columns, below) get exponent −1100 and scale 0: their values
         // become zero and are never stored
-        const bool rok = i < Mreal;
-        ei = rok ? max(eA[i], -1100) : -1100;
+        ei = rok ? max(eA_i, -1100) : -1100;
         // the row scale carries the recombination's 2^(−7(sb+1))
         const int eis = ei - 7 * (sb + 1);
         const double rscale = (eis >= -1022 && eis <= 1023) ? pow2i(eis) : 0.0;
         // lane l holds the exponent and scale of the warp's column 32·half + l (shared by shuffles)
-        const int64_t jl = it.n0 + 32 * half + lane;
-        const bool cok = jl < b.n;
-        const int ej = cok ? max(eB[jl], -1100) : -1100;
+        const int ej = cok ? max(eB_j, -1100) : -1100;
         const double cs = (ej >= -1022 && ej <= 1023) ? pow2i(ej) : 0.0;
         ejm = ej;
         // the exact (ldexp) scaling only where a real row's or column's 2^e is not a normal double
