@@ -760,10 +760,11 @@ def kernel_roofline(args, log, ctx, flush):
             ops = dom["int8_ops"]
             ach = ops / (dom["ms"] * 1e-3) / 1e12
             peak = 2.0 * bf16
-            roof = {"kernel": "gemm_split_fused_kernel (slicing + int8 tensor-core products + FP64 "
-                              "recombination, one launch)",
+            roof = {"kernel": "grouped split GEMM call: gemm_split_slice_kernel (slicing) + "
+                              "gemm_split_fused_kernel (int8 tensor-core products, FP64 recombination)",
                     "bound": "tensor", "achieved": ach, "peak": peak, "unit": "TFLOP/s",
-                    "frac": ach / peak, "traffic": profile_traffic("gemm_split_fused_su2_large"),
+                    "frac": ach / peak,
+                    "traffic": profile_traffic("gemm_split_fused_su2_large", "traffic_bytes_per_call"),
                     "peak_source": f"2 x bf16_tflops of {src} peaks (int8 dense = 2 x bf16 dense)",
                     "algorithmic": f"sum over blocks of S_b(S_b+1)/2 int8 products of 2mnk = {ops:.4e} "
                                    f"(slice counts {dom['block_slices']})",
@@ -774,12 +775,13 @@ def kernel_roofline(args, log, ctx, flush):
     return roof, rows
 
 
-def profile_traffic(name):
-    """DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum) of a kernel from its
-    committed ncu summary profiles/<name>.md (a line `traffic_bytes_per_launch: N`), else None."""
+def profile_traffic(name, key="traffic_bytes_per_launch"):
+    """DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of a kernel launch, or of the
+    launches of one library call, from the committed ncu summary profiles/<name>.md (a line
+    `<key>: N`), else None."""
     try:
         for ln in open(os.path.join(ROOT, "profiles", name + ".md")):
-            if ln.strip().startswith("traffic_bytes_per_launch:"):
+            if ln.strip().startswith(key + ":"):
                 return float(ln.split(":", 1)[1].split()[0])
     except (OSError, ValueError, IndexError):
         pass
