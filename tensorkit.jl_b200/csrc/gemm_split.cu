@@ -314,6 +314,10 @@ __device__ __forceinline__ void store_piece(const typename SrcVal<CPLX>::T (&v)[
 // exponent of op(A) rows and of op(B) columns, biased by kExpBias so that 0 means "no nonzero
 // row", and the largest row 2-norms as double bits)
 constexpr int kExpBias = 4096;
+// fire-and-forget maximum into global memory (no value returned, so nothing waits for it)
+__device__ __forceinline__ void red_max_u64(unsigned long long *p, unsigned long long v) {
+  asm volatile("red.relaxed.gpu.global.max.u64 [%0], %1;\n" ::"l"(p), "l"(v) : "memory");
+}
 
 __device__ __forceinline__ void fence_proxy_async_global() {
   asm volatile("fence.proxy.async.global;\n" ::: "memory");
@@ -399,8 +403,8 @@ __device__ __forceinline__ void slice_warp_task(const SliceTask &task, const voi
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) nrm = fmax(nrm, __shfl_xor_sync(full, nrm, o));
   if (lane == 0 && ebm != 0u) {
-    atomicMax(&bst[4 * task.block + op], (unsigned long long)ebm);
-    atomicMax(&bst[4 * task.block + 2 + op], (unsigned long long)__double_as_longlong(nrm));
+    red_max_u64(&bst[4 * task.block + op], (unsigned long long)ebm);
+    red_max_u64(&bst[4 * task.block + 2 + op], (unsigned long long)__double_as_longlong(nrm));
   }
 }
 
@@ -593,10 +597,10 @@ constexpr double kSliceMargin = 0.5;
 
 template <int SM>
 __device__ __forceinline__ int choose_slices(const unsigned long long *bst, int block, int64_t kpad) {
-  const unsigned long long ea = bst[4 * block], eb = bst[4 * block + 1];
+  const unsigned long long ea = __ldcg(&bst[4 * block]), eb = __ldcg(&bst[4 * block + 1]);
   if (ea == 0ull || eb == 0ull) return SM;  // an operand of the block is zero: so are its products
-  const double na = __longlong_as_double((long long)bst[4 * block + 2]);
-  const double nb = __longlong_as_double((long long)bst[4 * block + 3]);
+  const double na = __longlong_as_double((long long)__ldcg(&bst[4 * block + 2]));
+  const double nb = __longlong_as_double((long long)__ldcg(&bst[4 * block + 3]));
   const double k = (double)kpad;
   const double cmax = 4.5 * na * nb / sqrt(k);
   const int e = (int)ea + (int)eb - 2 * kExpBias;
@@ -755,8 +759,9 @@ struct FusedArgs {
   const double *A, *B;
   double *C;
   int8_t *ws;
-  int *cnt;                 // [0] slicing claims, [1] finished product CTAs, [2] tiles recomputed in
-                            // FP64, [3] finished slicing warps, [4 + slot] split-K arrivals
+  int *cnt;                 // [1] finished product CTAs, [2] tiles recomputed in FP64,
+                            // [4 + block] source rows sliced (both operands),
+                            // [4 + nblocks + block] the block's slice count + 1 (0: not yet sliced)
   unsigned long long *bst;  // 4 per block: statistics of the slicing
   int *slices_out;          // per block: the slice count of the last launch (0 = FP64, −1 = no
                             // products), then the number of tiles the check sent to FP64
@@ -765,6 +770,7 @@ struct FusedArgs {
   int *err;
   CDbl alpha, beta;
   int nstasks, nitems, nblocks;
+  int nctasks;              // the first nctasks slicing tasks are staged CTA tasks
   int fixed;                // 1: the caller fixed the slice count (every block uses S, no check)
 };
 
@@ -777,6 +783,22 @@ __device__ __forceinline__ bool mbar_wait_abortable(uint64_t *bar, uint32_t pari
     if (mbar_try(addr, parity)) return true;
     if (*abort) return false;
     if ((n & 63u) == 0 && globaltimer_ns() - t0 > 2000000000ull) return false;
+  }
+}
+__device__ __forceinline__ int ld_acquire(const int *p) {
+  int v;
+  asm volatile("ld.acquire.gpu.global.s32 %0, [%1];\n" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+// bounded wait until *p ≥ target (acquire at GPU scope); false once 2 s have passed or the CTA
+// aborts (a count already reached costs one load)
+__device__ __forceinline__ bool wait_at_least(const int *p, int target, const volatile int *abort) {
+  if (ld_acquire(p) >= target) return true;
+  const uint64_t t0 = globaltimer_ns();
+  while (true) {
+    __nanosleep(64);
+    if (ld_acquire(p) >= target) return true;
+    if (*abort || globaltimer_ns() - t0 > 2000000000ull) return false;
   }
 }
 __device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
@@ -947,13 +969,21 @@ __global__ void __launch_bounds__(kFusedThreads, 1) gemm_split_fused_kernel(cons
     const char *pb = reinterpret_cast<const char *>(g.blocks + it0.block);
     for (int o = 0; o < (int)sizeof(GBlock); o += 64) asm volatile("prefetch.L1 [%0];\n" ::"l"(pb + o));
   }
-  pdl_wait();  // the slicing launch has finished; C comes from earlier kernels of the stream
+  // No wait for the slicing launch to finish: every role waits for the readiness counts of its
+  // item's block instead (the slicing launch publishes each task's rows). This launch starts
+  // only once every CTA of the slicing launch runs (which in turn began after the earlier kernels
+  // of the stream had finished), so the counts always complete, and C and the FP64 operands are
+  // final.
+  int *ready = g.cnt + 4;  // [block]: source rows sliced (both operands); [nblocks + block]: slice count + 1
   if (tid == 0) TL_STAMP(1);
 
   // ---- products ------------------------------------------------------------------
   // a block's slice count (0: the block runs in FP64) from the statistics of the slicing launch
-  auto slices_of = [&](const GBlock &b, int block) -> int {
-    return b.fp64only ? 0 : g.fixed ? S : choose_slices<S>(g.bst, block, b.kpad);
+  // bounded wait until both operands of a block are sliced; the slicing task that completes the
+  // block publishes its slice count as sb + 1 (acquire: the slices, exponents and statistics of
+  // the block are visible after it). −1 on timeout or abort.
+  auto sliced = [&](int block) -> int {
+    return wait_at_least(&ready[g.nblocks + block], 1, abort) ? ld_acquire(&ready[g.nblocks + block]) - 1 : -1;
   };
   if (warp == kProducerWarp) {
     if (lane == 0) {
@@ -963,7 +993,12 @@ __global__ void __launch_bounds__(kFusedThreads, 1) gemm_split_fused_kernel(cons
         const SplitTile it = g.items[ii];
         if (it.kind != 0) continue;
         const GBlock b = g.blocks[it.block];
-        const int sb = slices_of(b, it.block);
+        const int sb = sliced(it.block);
+        if (sb < 0) {
+          atomicExch(g.err, 3);
+          *abort = 1;
+          break;
+        }
         if (issued == 0) TL_STAMP(7);
         if (sb == 0) continue;  // the block runs in FP64
         fence_proxy_async_global();
@@ -1002,7 +1037,12 @@ __global__ void __launch_bounds__(kFusedThreads, 1) gemm_split_fused_kernel(cons
       for (int k = 0, ii = item_of(0); ii < g.nitems && ok && !*abort; ii = item_of(++k)) {
         const SplitTile it = g.items[ii];
         if (it.kind != 0) continue;
-        const int sb = slices_of(g.blocks[it.block], it.block);
+        const int sb = sliced(it.block);
+        if (sb < 0) {
+          atomicExch(g.err, 3);
+          *abort = 1;
+          break;
+        }
         if (sb == 0) continue;
         if (li > 0 && !mbar_wait_abortable(acc_empty, (li - 1) & 1, abort)) {
           atomicExch(g.err, 2);
@@ -1077,7 +1117,16 @@ __global__ void __launch_bounds__(kFusedThreads, 1) gemm_split_fused_kernel(cons
       const int64_t i = it.m0 + row;
       const bool prod = it.kind == 0;
       bool stop = *abort != 0;
-      const int sb = prod ? slices_of(b, it.block) : 0;
+      int sb = 0;
+      if (prod && !stop) {
+        // lane 0 acquires the block's slice count; __syncwarp orders the other lanes' reads of the
+        // exponents after that acquire
+        if (lane == 0) sb = sliced(it.block);
+        __syncwarp();
+        sb = __shfl_sync(0xffffffffu, sb, 0);
+        stop = sb < 0;
+        if (stop) sb = 0;
+      }
       const bool mma = prod && sb > 0;  // the tile's products ran on the tensor cores
       // the row exponent and the exponent of this lane's column, read before the products finish
       const int32_t *eA = reinterpret_cast<const int32_t *>(g.ws + b.wsEA);
@@ -1307,11 +1356,12 @@ __global__ void __launch_bounds__(kFusedThreads, 1) gemm_split_fused_kernel(cons
       __threadfence();
       for (int q = lane; q < g.nblocks; q += 32) {
         const GBlock &b = g.blocks[q];
-        g.slices_out[q] = (b.m > 0 && b.n > 0 && b.k > 0 && !b.skinny) ? (g.fixed ? S : choose_slices<S>(g.bst, q, b.kpad))
-                                                                        : -1;
+        const int f = ready[g.nblocks + q];
+        g.slices_out[q] = (b.m > 0 && b.n > 0 && b.k > 0 && !b.skinny && f > 0) ? f - 1 : -1;
       }
       __syncwarp();
       for (int q = lane; q < 4 * g.nblocks; q += 32) g.bst[q] = 0ull;
+      for (int q = lane; q < 2 * g.nblocks; q += 32) ready[q] = 0;
       if (lane == 0) {
         g.slices_out[g.nblocks] = g.cnt[2];
         g.cnt[2] = 0;
@@ -1322,25 +1372,171 @@ __global__ void __launch_bounds__(kFusedThreads, 1) gemm_split_fused_kernel(cons
   }
 }
 
-// The slicing launch: warp w of the grid takes the tasks w, w + W, w + 2W, … (W warps; the
-// planner sorts the tasks largest first). Many warps per SM keep many piece loads in flight. It
-// lets the products launch start its prologue as soon as all its CTAs run; that launch waits for
-// it to finish before its first product.
+// Staged slicing task, run by the whole CTA (every thread calls): nrows whole rows of one operand
+// are copied into shared memory with cp.async (consecutive threads take consecutive addresses:
+// along the rows when the rows are contiguous in memory, along K otherwise), so a task costs one
+// memory round trip. Row maxima and sums of squares then come from shared memory (one warp per
+// row), and every thread slices pieces of 16 real (8 complex) K values out of it. A stage row
+// holds kfull values plus one padding value per piece (fewer bank conflicts between pieces).
+constexpr int kStageBytes = 48 * 1024;  // shared memory of one staged task
+constexpr int kStagedRowsMax = 64;      // rows of one staged task
+template <typename T>
+__device__ __forceinline__ void cp_async_elem(T *dst, const T *src) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], %2;\n" ::"r"(smem_u32(dst)), "l"(src), "n"(sizeof(T))
+               : "memory");
+}
+template <int S, bool CPLX, int NT>
+__device__ __forceinline__ void slice_staged(const SliceTask &task, const void *Xv, int8_t *ws, unsigned long long *bst,
+                                             void *stage_v, int *rexp) {
+  using T = typename SrcVal<CPLX>::T;
+  constexpr int LK = CPLX ? 8 : 16;
+  constexpr int NW = NT / 32;
+  const unsigned full = 0xffffffffu;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int op = task.operand;
+  const int64_t kfull = CPLX ? task.kpad / 2 : task.kpad;
+  const int nchunk = (int)(kfull / LK);
+  const int stride = (int)(kfull + kfull / LK);  // stage row length in elements (with padding)
+  const int nrows = task.nrows;
+  const bool rowc = task.rs == 1;
+  T *stage = reinterpret_cast<T *>(stage_v);
+  const T *X = reinterpret_cast<const T *>(Xv);
+  const T z = zero_of(T{});
+  // 1. copy the rows in (zeros past k and for rows past the operand)
+  const int total = nrows * (int)kfull;
+#pragma unroll 1
+  for (int q = tid; q < total; q += NT) {
+    int r, c;
+    if (rowc) {
+      r = q % nrows;
+      c = q / nrows;
+    } else {
+      c = q % (int)kfull;
+      r = q / (int)kfull;
+    }
+    T *dst = stage + r * stride + c + c / LK;
+    const int64_t rr = task.r0 + r;
+    if (c < task.k && rr < task.msrc) cp_async_elem(dst, X + task.xoff + rr * task.rs + (int64_t)c * task.ks);
+    else *dst = z;
+  }
+  asm volatile("cp.async.commit_group;\ncp.async.wait_all;\n" ::: "memory");
+  __syncthreads();
+  if (tid == 0) TL_STAMP(3);
+  // 2. row maxima, sums of squares, exponents (one warp per row)
+  unsigned ebm = 0u;
+  double nrm = 0.0;
+  int32_t *ex = reinterpret_cast<int32_t *>(ws + task.ws_e);
+#pragma unroll 1
+  for (int r = warp; r < nrows; r += NW) {
+    double m = 0.0, s2 = 0.0;
+    const T *row = stage + r * stride;
+#pragma unroll 4
+    for (int c = lane; c < (int)kfull; c += 32) {
+      const T v = row[c + c / LK];
+      m = fmax(m, absmax(v));
+      s2 += sq_of(v);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      m = fmax(m, __shfl_xor_sync(full, m, o));
+      s2 += __shfl_xor_sync(full, s2, o);
+    }
+    const int e = row_exponent<S>(m);
+    const int64_t rr = task.r0 + r;
+    if (lane == 0) {
+      rexp[r] = e;
+      if (rr < task.msrc) {
+        if (CPLX && op == 0) {
+          ex[2 * rr] = e;
+          ex[2 * rr + 1] = e;
+        } else {
+          ex[rr] = e;
+        }
+      }
+    }
+    if (rr < task.msrc && m > 0.0) {
+      ebm = max(ebm, (unsigned)(e + kExpBias));
+      nrm = fmax(nrm, sqrt(s2));
+    }
+  }
+  if (lane == 0 && ebm != 0u) {
+    red_max_u64(&bst[4 * task.block + op], (unsigned long long)ebm);
+    red_max_u64(&bst[4 * task.block + 2 + op], (unsigned long long)__double_as_longlong(nrm));
+  }
+  __syncthreads();
+  if (tid == 0) TL_STAMP(4);
+  // 3. the slices of every piece (row, p)
+  int8_t *base = ws + task.ws_s;
+  const int npieces = nrows * nchunk;
+#pragma unroll 1
+  for (int q = tid; q < npieces; q += NT) {
+    const int r = q / nchunk, p = q - r * nchunk;
+    const int64_t rr = task.r0 + r;
+    if (rr >= task.msrc) continue;
+    const T *src = stage + r * stride + p * (LK + 1);
+    T v[LK];
+#pragma unroll
+    for (int l = 0; l < LK; ++l) v[l] = src[l];
+    store_piece<S, CPLX, LK>(v, op, task.conj != 0, rr, (int64_t)p * LK, kfull, task.kpad, base, rexp[r]);
+  }
+  __syncthreads();  // the stage and rexp are rewritten by the next task
+  if (tid == 0) TL_STAMP(5);
+}
+
+// The slicing launch: the staged CTA tasks (the first nctasks) go to the CTAs in turn, then warp w
+// of the grid takes the warp tasks w, w + W, … (W warps); each list is sorted largest first. Every
+// task publishes its rows on the readiness count of its (block, operand). The launch lets the
+// products launch start as soon as all its CTAs run; the products wait for the counts of their
+// blocks, not for this launch to finish.
+// Called by one thread once a task's slices, exponents and statistics are written (and fenced
+// for the async proxy): adds the task's rows to its block's count; the task that completes the
+// block (both operands) sets the block's slice count from the statistics and publishes it as
+// slice count + 1 (release), which the products launch waits for.
+template <int S>
+__device__ __forceinline__ void publish_rows(const FusedArgs &g, const SliceTask &task) {
+  __threadfence();
+  const GBlock &b = g.blocks[task.block];
+  const int old = atomicAdd(&g.cnt[4 + task.block], task.nrows);
+  if (old + task.nrows == (int)(b.m + b.n)) {
+    __threadfence();  // acquire: every task's statistics of the block are visible
+    const int sb = b.fp64only ? 0 : g.fixed ? S : choose_slices<S>(g.bst, task.block, b.kpad);
+    asm volatile("st.release.gpu.global.s32 [%0], %1;\n" ::"l"(&g.cnt[4 + g.nblocks + task.block]), "r"(sb + 1)
+                 : "memory");
+  }
+}
 constexpr int kSliceThreads = 256;
 template <int S, bool CPLX>
 __global__ void __launch_bounds__(kSliceThreads, 2) gemm_split_slice_kernel(const FusedArgs args) {
+  extern __shared__ __align__(16) unsigned char stage[];
+  __shared__ int rexp[kStagedRowsMax];
   const FusedArgs &g = args;
   pdl_wait();     // the operands come from earlier kernels of the stream
   pdl_trigger();  // the products launch may begin its prologue
   const int lane = threadIdx.x & 31;
   if (threadIdx.x == 0) TL_STAMP(28);
+#pragma unroll 1
+  for (int t = (int)blockIdx.x; t < g.nctasks; t += (int)gridDim.x) {
+    const SliceTask task = g.stasks[t];
+    slice_staged<S, CPLX, kSliceThreads>(task, task.operand == 0 ? (const void *)g.A : (const void *)g.B, g.ws,
+                                         g.bst, stage, rexp);
+    // publish the task's rows: the slices are read by bulk copies (async proxy) of the products
+    fence_proxy_async_global();
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      publish_rows<S>(g, task);
+      TL_ADD(30, 1);
+    }
+  }
   const int nw = (int)gridDim.x * (kSliceThreads / 32);
-  for (int t = (int)blockIdx.x * (kSliceThreads / 32) + (int)(threadIdx.x >> 5); t < g.nstasks; t += nw) {
+  for (int t = g.nctasks + (int)blockIdx.x * (kSliceThreads / 32) + (int)(threadIdx.x >> 5); t < g.nstasks; t += nw) {
     const SliceTask task = g.stasks[t];
     const void *X = task.operand == 0 ? (const void *)g.A : (const void *)g.B;
     [[maybe_unused]] const unsigned long long t0 = TL_NOW();
     slice_warp_task<S, CPLX>(task, X, g.ws, g.bst);
+    fence_proxy_async_global();
+    __syncwarp();
     if (lane == 0) {
+      publish_rows<S>(g, task);
       TL_ADD(30, 1);
       TL_MAX(31, TL_NOW() - t0);
     }
@@ -1374,6 +1570,7 @@ int launch_split(tkb_ctx *ctx, const tkb_plan *p, void *C, const void *A, const 
   fa.alpha = a;
   fa.beta = b;
   fa.nstasks = (int)p->nsrows;
+  fa.nctasks = (int)p->nsctasks;
   fa.nitems = (int)p->nkstiles;
   fa.nblocks = (int)p->hblocks.size();
   fa.fixed = p->slices_fixed;
@@ -1384,9 +1581,12 @@ int launch_split(tkb_ctx *ctx, const tkb_plan *p, void *C, const void *A, const 
   TKB_CUDA_TRY(ctx, cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   if (fa.nstasks > 0) {
     auto ks = cplx ? gemm_split_slice_kernel<S, true> : gemm_split_slice_kernel<S, false>;
+    TKB_CUDA_TRY(ctx, cudaFuncSetAttribute(ks, cudaFuncAttributeMaxDynamicSharedMemorySize, kStageBytes));
+    // one CTA per staged task and one warp per warp task, where that fits two CTAs per SM
     const int warps = kSliceThreads / 32;
-    const int grid = std::max(1, std::min(2 * ctx->num_sms, (fa.nstasks + warps - 1) / warps));
-    TKB_CUDA_TRY(ctx, launch_pdl(ks, dim3((unsigned)grid), dim3(kSliceThreads), 0, ctx->stream, fa));
+    const int grid = std::max(1, std::min(2 * ctx->num_sms,
+                                          std::max(fa.nctasks, (fa.nstasks - fa.nctasks + warps - 1) / warps)));
+    TKB_CUDA_TRY(ctx, launch_pdl(ks, dim3((unsigned)grid), dim3(kSliceThreads), (size_t)kStageBytes, ctx->stream, fa));
     ctx->launches++;
   }
   // two-CTA clusters, as many as can be resident at once (the persistent loop takes the rest)
@@ -1476,17 +1676,28 @@ int tkb_gemm_split_prepare(tkb_ctx *ctx, tkb_plan *p) {
     for (int64_t m0 = 0; m0 < M; m0 += PANEL_A)
       for (int64_t n0 = 0; n0 < b.n; n0 += PANEL_B) tiles.push_back({(int32_t)bi, (int32_t)m0, (int32_t)n0, kind});
   }
-  // slicing tasks (one warp each): about kTaskPieces pieces of whole rows, in multiples of the
-  // rows one pass of the warp takes, halved while there would be fewer than 16 tasks per SM. Only the operands' own rows are sliced: padding rows of a panel
-  // feed output rows and columns that are never stored.
-  std::vector<SliceTask> jobs;
-  if (!sj.empty()) {
-    for (int div = 1;; div *= 2) {
-      jobs.clear();
-      for (const SJob &t : sj) {
-        const int64_t R = 32 / slice_groups(t.nchunk);
-        const int64_t passes = std::max<int64_t>(1, kTaskPieces / (R * std::max<int32_t>(1, t.nchunk)) / div);
-        const int32_t r = (int32_t)(R * passes);
+  // slicing tasks. Rows whose K values fit the stage go to staged CTA tasks of up to
+  // kStagedRowsMax rows and kStageBytes of values, made smaller (down to one row) while there would
+  // be fewer tasks than two per SM; longer rows go to warp tasks (about kTaskPieces pieces of whole
+  // rows, in multiples of the rows one pass of the warp takes). CTA tasks come first; each list is
+  // sorted largest first. Only the operands' own rows are sliced: padding rows of a panel feed
+  // output rows and columns that are never stored.
+  std::vector<SliceTask> jobs, wjobs;
+  {
+    const int64_t esize = cplx ? 16 : 8;
+    int64_t staged_bytes = 0;
+    for (const SJob &t : sj) {
+      const int64_t kfull = cplx ? p->hblocks[t.block].kpad / 2 : p->hblocks[t.block].kpad;
+      const int64_t rowb = (kfull + kfull / (cplx ? 8 : 16)) * esize;
+      if (rowb <= kStageBytes) staged_bytes += rowb * t.nsrc;
+    }
+    const int64_t per_task = std::max<int64_t>(8 * 1024, staged_bytes / std::max<int64_t>(1, 2 * ctx->num_sms));
+    for (const SJob &t : sj) {
+      const int64_t kfull = cplx ? p->hblocks[t.block].kpad / 2 : p->hblocks[t.block].kpad;
+      const int64_t rowb = (kfull + kfull / (cplx ? 8 : 16)) * esize;
+      if (rowb <= kStageBytes) {
+        const int32_t r = (int32_t)std::max<int64_t>(
+            1, std::min<int64_t>({(int64_t)kStagedRowsMax, kStageBytes / rowb, (per_task + rowb - 1) / rowb}));
         for (int32_t r0 = 0; r0 < t.nsrc; r0 += r) {
           SliceTask j{};
           j.block = t.block;
@@ -1495,15 +1706,26 @@ int tkb_gemm_split_prepare(tkb_ctx *ctx, tkb_plan *p) {
           j.nrows = std::min(r, t.nsrc - r0);
           jobs.push_back(j);
         }
+      } else {
+        const int64_t R = 32 / slice_groups(t.nchunk);
+        const int64_t passes = std::max<int64_t>(1, kTaskPieces / (R * std::max<int32_t>(1, t.nchunk)));
+        const int32_t r = (int32_t)(R * passes);
+        for (int32_t r0 = 0; r0 < t.nsrc; r0 += r) {
+          SliceTask j{};
+          j.block = t.block;
+          j.operand = t.op;
+          j.r0 = r0;
+          j.nrows = std::min(r, t.nsrc - r0);
+          wjobs.push_back(j);
+        }
       }
-      if ((int64_t)jobs.size() >= 16 * (int64_t)ctx->num_sms || div >= 64) break;
     }
-    // the tasks with the most pieces first
-    std::vector<int32_t> nch(p->hblocks.size(), 0);
-    for (const SJob &t : sj) nch[t.block] = t.nchunk;
-    std::stable_sort(jobs.begin(), jobs.end(), [&](const SliceTask &x, const SliceTask &y) {
-      return (int64_t)x.nrows * nch[x.block] > (int64_t)y.nrows * nch[y.block];
-    });
+    auto cost = [&](const SliceTask &x) { return (int64_t)x.nrows * p->hblocks[x.block].kpad; };
+    auto larger = [&](const SliceTask &x, const SliceTask &y) { return cost(x) > cost(y); };
+    std::stable_sort(jobs.begin(), jobs.end(), larger);
+    std::stable_sort(wjobs.begin(), wjobs.end(), larger);
+    p->nsctasks = (int64_t)jobs.size();
+    jobs.insert(jobs.end(), wjobs.begin(), wjobs.end());
   }
   // exponent arrays of every block in one contiguous region (rewritten by every launch)
   p->expo_off = (int64_t)off;
@@ -1607,7 +1829,7 @@ int tkb_gemm_split_prepare(tkb_ctx *ctx, tkb_plan *p) {
   // claim, finish, check and slicing-warp counts, then one split-K arrival counter per split
   // tile; the block statistics; the per-block slice counts of the last launch
   const size_t nb = p->hblocks.size();
-  const size_t ncnt = 4 + (size_t)nslots;
+  const size_t ncnt = 4 + 2 * nb + (size_t)nslots;
   if (e == cudaSuccess) e = cudaMalloc((void **)&p->pcnt, ncnt * sizeof(int));
   if (e == cudaSuccess) e = cudaMemset(p->pcnt, 0, ncnt * sizeof(int));
   if (e == cudaSuccess) e = cudaMalloc((void **)&p->bstat, std::max<size_t>(1, 4 * nb) * sizeof(unsigned long long));

@@ -222,6 +222,7 @@ struct tkb_plan {
   int slices_fixed = 0;         // split: the caller fixed the slice count
   void *sjobs = nullptr;        // slicing tasks (block, operand, rows)
   int64_t nsrows = 0;           // slicing tasks
+  int64_t nsctasks = 0;         // of which the first are staged (one CTA each)
   int tile_m = 64, tile_n = 64;
   // split-K knobs (tkb_gemm_plan_create_tuned): pieces per tile at most, K steps per piece at least
   int max_pieces = 8, min_piece_steps = 4;
