@@ -1422,15 +1422,19 @@ __device__ __forceinline__ void slice_staged(const SliceTask &task, const void *
   const T z = zero_of(T{});
   // 1. copy the rows in (zeros past k and for rows past the operand)
   const int total = nrows * (int)kfull;
+  // element q = tid, tid + NT, … as (r, c): the fast index (r for row-contiguous, c otherwise)
+  // steps by NT mod fast with a carry into the slow one (no division per element)
+  const int fast = rowc ? nrows : (int)kfull;
+  const int fstep = NT % fast, sstep = NT / fast;
+  int fi = tid % fast, si = tid / fast;
 #pragma unroll 1
   for (int q = tid; q < total; q += NT) {
-    int r, c;
-    if (rowc) {
-      r = q % nrows;
-      c = q / nrows;
-    } else {
-      c = q % (int)kfull;
-      r = q / (int)kfull;
+    const int r = rowc ? fi : si, c = rowc ? si : fi;
+    fi += fstep;
+    si += sstep;
+    if (fi >= fast) {
+      fi -= fast;
+      ++si;
     }
     T *dst = stage + r * stride + c + c / LK;
     const int64_t rr = task.r0 + r;
@@ -1486,16 +1490,24 @@ __device__ __forceinline__ void slice_staged(const SliceTask &task, const void *
   // 3. the slices of every piece (row, p)
   int8_t *base = ws + task.ws_s;
   const int npieces = nrows * nchunk;
+  const int pstep = NT % nchunk, rstep = NT / nchunk;
+  int p = tid % nchunk, r = tid / nchunk;
 #pragma unroll 1
   for (int q = tid; q < npieces; q += NT) {
-    const int r = q / nchunk, p = q - r * nchunk;
-    const int64_t rr = task.r0 + r;
+    const int pr = p, rr0 = r;
+    p += pstep;
+    r += rstep;
+    if (p >= nchunk) {
+      p -= nchunk;
+      ++r;
+    }
+    const int64_t rr = task.r0 + rr0;
     if (rr >= task.msrc) continue;
-    const T *src = stage + r * stride + p * (LK + 1);
+    const T *src = stage + rr0 * stride + pr * (LK + 1);
     T v[LK];
 #pragma unroll
     for (int l = 0; l < LK; ++l) v[l] = src[l];
-    store_piece<S, CPLX, LK>(v, op, task.conj != 0, rr, (int64_t)p * LK, kfull, task.kpad, base, rexp[r]);
+    store_piece<S, CPLX, LK>(v, op, task.conj != 0, rr, (int64_t)pr * LK, kfull, task.kpad, base, rexp[rr0]);
   }
   __syncthreads();  // the stage and rexp are rewritten by the next task
   if (tid == 0) TL_STAMP(5);
@@ -1512,11 +1524,15 @@ __device__ __forceinline__ void slice_staged(const SliceTask &task, const void *
 // slice count + 1 (release), which the products launch waits for.
 template <int S>
 __device__ __forceinline__ void publish_rows(const FusedArgs &g, const SliceTask &task) {
-  __threadfence();
   const GBlock &b = g.blocks[task.block];
-  const int old = atomicAdd(&g.cnt[4 + task.block], task.nrows);
+  // one acquire-release add: releases this task's writes (the CTA's, ordered by the barrier before
+  // the call) and, for the task that completes the block, acquires every other task's statistics
+  int old;
+  asm volatile("atom.acq_rel.gpu.global.add.s32 %0, [%1], %2;\n"
+               : "=r"(old)
+               : "l"(&g.cnt[4 + task.block]), "r"(task.nrows)
+               : "memory");
   if (old + task.nrows == (int)(b.m + b.n)) {
-    __threadfence();  // acquire: every task's statistics of the block are visible
     const int sb = b.fp64only ? 0 : g.fixed ? S : choose_slices<S>(g.bst, task.block, b.kpad);
     asm volatile("st.release.gpu.global.s32 [%0], %1;\n" ::"l"(&g.cnt[4 + g.nblocks + task.block]), "r"(sb + 1)
                  : "memory");
