@@ -269,7 +269,7 @@ __device__ __forceinline__ void store_piece(const typename SrcVal<CPLX>::T (&v)[
     for (int q = 0; q < LK; ++q) x[q] = to_fixed(v[q], rsc);
     sign_masks([&](int q) { return v[q]; }, M);
     int8_t *p = base + slice_off(r, c, kpad, pr, S);
-#pragma unroll 1
+#pragma unroll
     for (int sl = 0; sl < S; ++sl) *reinterpret_cast<P *>(p + sl * plane) = slice_piece<S, LK>(x, M, sl);
   } else {
     Fixed xr[LK], xi[LK];
@@ -288,7 +288,7 @@ __device__ __forceinline__ void store_piece(const typename SrcVal<CPLX>::T (&v)[
       int8_t *p1 = base + slice_off(2 * r, kfull + c, kpad, pr, S);
       int8_t *p2 = base + slice_off(2 * r + 1, c, kpad, pr, S);
       int8_t *p3 = base + slice_off(2 * r + 1, kfull + c, kpad, pr, S);
-#pragma unroll 1
+#pragma unroll
       for (int sl = 0; sl < S; ++sl) {
         const P ur = slice_piece<S, LK>(xr, Mr, sl);
         const int64_t o = sl * plane;
@@ -300,7 +300,7 @@ __device__ __forceinline__ void store_piece(const typename SrcVal<CPLX>::T (&v)[
     } else {  // column j of op(B): [Re | Im]
       int8_t *p0 = base + slice_off(r, c, kpad, pr, S);
       int8_t *p1 = base + slice_off(r, kfull + c, kpad, pr, S);
-#pragma unroll 1
+#pragma unroll
       for (int sl = 0; sl < S; ++sl) {
         const int64_t o = sl * plane;
         *reinterpret_cast<P *>(p0 + o) = slice_piece<S, LK>(xr, Mr, sl);
@@ -1405,7 +1405,7 @@ __device__ __forceinline__ void cp_async_elem(T *dst, const T *src) {
 }
 template <int S, bool CPLX, int NT>
 __device__ __forceinline__ void slice_staged(const SliceTask &task, const void *Xv, int8_t *ws, unsigned long long *bst,
-                                             void *stage_v, int *rexp) {
+                                             void *stage_v, int *rexp, unsigned long long *wstat) {
   using T = typename SrcVal<CPLX>::T;
   constexpr int LK = CPLX ? 8 : 16;
   constexpr int NW = NT / 32;
@@ -1444,28 +1444,33 @@ __device__ __forceinline__ void slice_staged(const SliceTask &task, const void *
   asm volatile("cp.async.commit_group;\ncp.async.wait_all;\n" ::: "memory");
   __syncthreads();
   if (tid == 0) TL_STAMP(3);
-  // 2. row maxima, sums of squares, exponents (one warp per row)
+  // 2. row maxima, sums of squares, exponents: eight lanes per row, four rows per warp at a time
   unsigned ebm = 0u;
   double nrm = 0.0;
   int32_t *ex = reinterpret_cast<int32_t *>(ws + task.ws_e);
+  const int sub = lane >> 3, l8 = lane & 7;
 #pragma unroll 1
-  for (int r = warp; r < nrows; r += NW) {
+  for (int r0 = 4 * warp; r0 < nrows; r0 += 4 * NW) {
+    const int r = r0 + sub;
     double m = 0.0, s2 = 0.0;
-    const T *row = stage + r * stride;
+    if (r < nrows) {
+      const T *row = stage + r * stride;
 #pragma unroll 4
-    for (int c = lane; c < (int)kfull; c += 32) {
-      const T v = row[c + c / LK];
-      m = fmax(m, absmax(v));
-      s2 += sq_of(v);
+      for (int c = l8; c < (int)kfull; c += 8) {
+        const T v = row[c + c / LK];
+        m = fmax(m, absmax(v));
+        s2 += sq_of(v);
+      }
     }
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
+    for (int o = 4; o > 0; o >>= 1) {
       m = fmax(m, __shfl_xor_sync(full, m, o));
       s2 += __shfl_xor_sync(full, s2, o);
     }
+    if (r >= nrows) continue;
     const int e = row_exponent<S>(m);
     const int64_t rr = task.r0 + r;
-    if (lane == 0) {
+    if (l8 == 0) {
       rexp[r] = e;
       if (rr < task.msrc) {
         if (CPLX && op == 0) {
@@ -1481,9 +1486,15 @@ __device__ __forceinline__ void slice_staged(const SliceTask &task, const void *
       nrm = fmax(nrm, sqrt(s2));
     }
   }
-  if (lane == 0 && ebm != 0u) {
-    red_max_u64(&bst[4 * task.block + op], (unsigned long long)ebm);
-    red_max_u64(&bst[4 * task.block + 2 + op], (unsigned long long)__double_as_longlong(nrm));
+  // the task's block statistics: one value per warp into shared memory, one reduction per task
+  // into the block statistics after the slices (the global reductions of many CTAs onto a few
+  // addresses stay out of the way of the loads and stores)
+  ebm = __reduce_max_sync(full, ebm);
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) nrm = fmax(nrm, __shfl_xor_sync(full, nrm, o));
+  if (lane == 0) {
+    wstat[warp] = ebm;
+    wstat[NW + warp] = (unsigned long long)__double_as_longlong(nrm);
   }
   __syncthreads();
   if (tid == 0) TL_STAMP(4);
@@ -1509,7 +1520,19 @@ __device__ __forceinline__ void slice_staged(const SliceTask &task, const void *
     for (int l = 0; l < LK; ++l) v[l] = src[l];
     store_piece<S, CPLX, LK>(v, op, task.conj != 0, rr, (int64_t)pr * LK, kfull, task.kpad, base, rexp[rr0]);
   }
-  __syncthreads();  // the stage and rexp are rewritten by the next task
+  if (tid == 0) {
+    unsigned long long e8 = 0ull, n8 = 0ull;
+#pragma unroll
+    for (int w = 0; w < NW; ++w) {
+      e8 = max(e8, wstat[w]);
+      n8 = max(n8, wstat[NW + w]);  // bits of non-negative doubles order like their values
+    }
+    if (e8 != 0ull) {
+      red_max_u64(&bst[4 * task.block + op], e8);
+      red_max_u64(&bst[4 * task.block + 2 + op], n8);
+    }
+  }
+  __syncthreads();  // the stage, rexp and wstat are rewritten by the next task
   if (tid == 0) TL_STAMP(5);
 }
 
@@ -1543,6 +1566,7 @@ template <int S, bool CPLX>
 __global__ void __launch_bounds__(kSliceThreads, 2) gemm_split_slice_kernel(const FusedArgs args) {
   extern __shared__ __align__(16) unsigned char stage[];
   __shared__ int rexp[kStagedRowsMax];
+  __shared__ unsigned long long wstat[2 * (kSliceThreads / 32)];
   const FusedArgs &g = args;
   pdl_wait();     // the operands come from earlier kernels of the stream
   pdl_trigger();  // the products launch may begin its prologue
@@ -1552,7 +1576,7 @@ __global__ void __launch_bounds__(kSliceThreads, 2) gemm_split_slice_kernel(cons
   for (int t = (int)blockIdx.x; t < g.nctasks; t += (int)gridDim.x) {
     const SliceTask task = g.stasks[t];
     slice_staged<S, CPLX, kSliceThreads>(task, task.operand == 0 ? (const void *)g.A : (const void *)g.B, g.ws,
-                                         g.bst, stage, rexp);
+                                         g.bst, stage, rexp, wstat);
     // publish the task's rows: the slices are read by bulk copies (async proxy) of the products
     fence_proxy_async_global();
     __syncthreads();
