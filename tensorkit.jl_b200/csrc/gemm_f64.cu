@@ -61,6 +61,14 @@ __device__ __forceinline__ void dmma(double &c0, double &c1, double a, double b)
                : "+d"(c0), "+d"(c1)
                : "d"(a), "d"(b));
 }
+// D(16×8) += A(16×8) B(8×8), FP64. Lane (g = lane/4, t = lane%4): a = A[g][t], A[g+8][t],
+// A[g][t+4], A[g+8][t+4]; b = B[t][g], B[t+4][g]; c = D[g][2t], D[g][2t+1], D[g+8][2t],
+// D[g+8][2t+1] (checked against a host product on the device)
+__device__ __forceinline__ void dmma16(double (&c)[4], const double (&a)[4], const double (&b)[2]) {
+  asm volatile("mma.sync.aligned.m16n8k8.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, {%0,%1,%2,%3};\n"
+               : "+d"(c[0]), "+d"(c[1]), "+d"(c[2]), "+d"(c[3])
+               : "d"(a[0]), "d"(a[1]), "d"(a[2]), "d"(a[3]), "d"(b[0]), "d"(b[1]));
+}
 
 // ---- real ----------------------------------------------------------------------------
 struct SmemR {
@@ -218,23 +226,35 @@ __global__ void __launch_bounds__(kRealThreads, 3)
       k_loop(task.kb, task.ke,
              [&](int st, int64_t k0) { load_tiles_r(s, st, b, A, B, m0, n0, k0, vec); },
              [&](int st) {
+               // the warp's 32×32 as 2 × 4 blocks of 16×8 (m16n8k8), K in steps of 8
 #pragma unroll
-               for (int kk = 0; kk < BK; kk += 4) {
-                 double af[4], bf[4];
+               for (int kk = 0; kk < BK; kk += 8) {
+                 double af[2][4], bf[4][2];
 #pragma unroll
-                 for (int mi = 0; mi < 4; ++mi) af[mi] = s.A[st][kk + t][wm * 32 + mi * 8 + g];
+                 for (int mi = 0; mi < 2; ++mi) {
+                   const int r = wm * 32 + mi * 16 + g;
+                   af[mi][0] = s.A[st][kk + t][r];
+                   af[mi][1] = s.A[st][kk + t][r + 8];
+                   af[mi][2] = s.A[st][kk + t + 4][r];
+                   af[mi][3] = s.A[st][kk + t + 4][r + 8];
+                 }
 #pragma unroll
-                 for (int ni = 0; ni < 4; ++ni) bf[ni] = s.B[st][wn * 32 + ni * 8 + g][kk + t];
+                 for (int ni = 0; ni < 4; ++ni) {
+                   bf[ni][0] = s.B[st][wn * 32 + ni * 8 + g][kk + t];
+                   bf[ni][1] = s.B[st][wn * 32 + ni * 8 + g][kk + t + 4];
+                 }
 #pragma unroll
-                 for (int mi = 0; mi < 4; ++mi)
+                 for (int mi = 0; mi < 2; ++mi)
 #pragma unroll
-                   for (int ni = 0; ni < 4; ++ni) dmma(acc[(mi * 4 + ni) * 2], acc[(mi * 4 + ni) * 2 + 1], af[mi], bf[ni]);
+                   for (int ni = 0; ni < 4; ++ni)
+                     dmma16(*reinterpret_cast<double(*)[4]>(&acc[(mi * 4 + ni) * 4]), af[mi], bf[ni]);
                }
              });
     }
     if (!splitk_reduce<32, kRealThreads>(task, acc, part, pcnt, &ticket)) continue;
-    // epilogue: C = α·acc + β·C, in four row groups (the old values of a group are loaded before
-    // its first store)
+    // epilogue: C = α·acc + β·C, in four row groups of 8 (the old values of a group are loaded
+    // before its first store). Row group R, value q (column block q/2, column 2t + q%2) is
+    // acc[((R/2)·4 + q/2)·4 + (R%2)·2 + q%2] (the m16n8k8 fragments)
 #pragma unroll
     for (int mi = 0; mi < 4; ++mi) {
       const int64_t i = m0 + wm * 32 + mi * 8 + g;
@@ -248,7 +268,7 @@ __global__ void __launch_bounds__(kRealThreads, 3)
       for (int q = 0; q < 8; ++q) {
         const int64_t j = n0 + wn * 32 + (q / 2) * 8 + 2 * t + (q % 2);
         if (i < b.m && j < b.n) {
-          double r = alpha * acc[mi * 8 + q];
+          double r = alpha * acc[((mi >> 1) * 4 + (q >> 1)) * 4 + (mi & 1) * 2 + (q & 1)];
           if (beta != 0.0) r = fma(beta, old[q], r);
           C[b.offC + i + j * b.ldc] = r;
         }
