@@ -1,9 +1,9 @@
 // Plain FP64 / ComplexF64 grouped block GEMM: one launch for all coupled-sector blocks of a
 // TensorKit mul! (src/tensors/linalg.jl:330-370).
 //
-// Tensor path: FP64 DMMA (mma.sync.m8n8k4.f64). tcgen05 has no f64 kind, so the
-// double-precision tensor pipe is reached through DMMA; the split-precision path
-// (gemm_split.cu) is the tcgen05 one.
+// Tensor path: FP64 DMMA (mma.sync m16n8k8 for real data, m8n8k4 for complex). tcgen05 has no
+// f64 kind, so the double-precision tensor pipe is reached through DMMA; the split-precision
+// path (gemm_split.cu) is the tcgen05 one.
 //
 // Work decomposition: 64×64 output tiles; when the tiles would leave resident CTA slots idle,
 // the K loops of the longest tiles are cut into pieces (split K) so that the pieces fill about
@@ -12,12 +12,17 @@
 // tile stores its FP64 partial tile; the piece that arrives last on the tile's counter adds all
 // partials in piece order (deterministic, no piece waits for another) and applies α, β.
 //
-// CTA: 4 warps in a 2×2 grid (each 32×32 = 4×4 DMMA tiles), BK = 16, a three-stage cp.async
-// ring (two stages in flight while one is consumed; one barrier per K step). Operand tiles are
-// copied in 16-byte pairs when the block's layout keeps pairs aligned (op N, even offsets and
-// leading dimensions, 16-byte aligned base), else in 8-byte elements; elements outside the block
-// are zero-filled, so any lda/offset parity works. Complex blocks copy whole 16-byte elements and
-// issue four real DMMA per fragment pair.
+// Real CTA: 4 warps in a 2×2 grid (each 32×32 = 2×4 m16n8k8 tiles, two accumulator sets: one
+// per K sub-step of 8), BK = 16, a three-stage cp.async ring (two stages in flight while one is
+// consumed; one barrier per K step; a stage's DMMA are issued before the refill copies).
+// Operand tiles are copied in 16-byte pairs when the block's layout keeps pairs aligned (op N,
+// even offsets and leading dimensions, 16-byte aligned base), else in 8-byte elements; elements
+// outside the block are zero-filled, so any lda/offset parity works. Complex blocks copy whole
+// 16-byte elements and issue four real DMMA per fragment pair.
+//
+// What bounds it: the DMMA pipe runs m16n8k8 at 64 cycles per SM sub-partition (37 TFLOP/s
+// measured on B200); the per-thread cp.async copies of a 16 KB stage cost the SM about a third
+// of that again (per-instruction load/store-unit work), so large blocks reach about 30 TFLOP/s.
 #include <algorithm>
 #include <cstring>
 
@@ -55,6 +60,28 @@ __device__ __forceinline__ void cp_async16(void *smem, const void *gmem, int byt
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
 template <int N>
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N)); }
+
+// Timeline build (-DTKB_TIMELINE): per CTA of the real kernel, global-timer stamps (ns) at entry
+// (0), after the grid-dependency wait (1), after the first task's K loop (2) and split-K
+// arrival (3), at exit (4); slot 5 counts the CTA's tasks, slot 6 holds the first task's
+// pieces and whether it was the last to arrive (2·nsplit + last). Read with
+// tkb_timeline_read_plain; the default build compiles every stamp away.
+#ifdef TKB_TIMELINE
+constexpr int kPlTlCtas = 512, kPlTlSlots = 8;
+__device__ unsigned long long tkb_tl_plain[kPlTlCtas * kPlTlSlots];
+__device__ __forceinline__ unsigned long long pl_now() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;\n" : "=l"(t));
+  return t;
+}
+#define PL_SET(k, v)                                                                         \
+  do {                                                                                       \
+    if (threadIdx.x == 0 && blockIdx.x < kPlTlCtas) tkb_tl_plain[blockIdx.x * kPlTlSlots + (k)] = (v); \
+  } while (0)
+#else
+#define PL_SET(k, v) ((void)0)
+#endif
+#define PL_STAMP(k) PL_SET(k, pl_now())
 
 __device__ __forceinline__ void dmma(double &c0, double &c1, double a, double b) {
   asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
@@ -149,24 +176,26 @@ __device__ __forceinline__ int vec_flags(const GBlock &b, int base_ok) {
   return v;
 }
 
-// K loop of one task through the NST-stage ring: `load(st, k0)` fills ring slot st with the
+// K loop of one task through an NS-stage ring: `load(st, k0)` fills ring slot st with the
 // tiles at K offset k0, `step(st)` consumes slot st. Every iteration commits one group (possibly
-// empty), so wait_group<NST-2> always means "the group of this iteration's stage has landed".
-template <typename Load, typename Step>
+// empty), so wait_group<NS-2> always means "the group of this iteration's stage has landed".
+template <int NS, typename Load, typename Step>
 __device__ __forceinline__ void k_loop(int kb, int ke, Load &&load, Step &&step) {
   const int nk = ke - kb;
 #pragma unroll
-  for (int st = 0; st < NST - 1; ++st) {
+  for (int st = 0; st < NS - 1; ++st) {
     if (st < nk) load(st, (int64_t)(kb + st) * BK);
     cp_async_commit();
   }
   for (int kt = 0; kt < nk; ++kt) {
-    cp_async_wait<NST - 2>();
+    cp_async_wait<NS - 2>();
     __syncthreads();  // stage kt visible to all; every warp is done with stage kt-1's slot
-    const int nxt = kt + NST - 1;
-    if (nxt < nk) load(nxt % NST, (int64_t)(kb + nxt) * BK);
+    const int nxt = kt + NS - 1;
+    // this stage's DMMA first, then the refill of the slot read in the previous iteration: the
+    // copies are issued while the DMMA execute
+    step(kt % NS);
+    if (nxt < nk) load(nxt % NS, (int64_t)(kb + nxt) * BK);
     cp_async_commit();
-    step(kt % NST);
   }
   cp_async_wait<0>();
   __syncthreads();  // the ring may be refilled by the next task
@@ -202,33 +231,39 @@ __device__ __forceinline__ bool splitk_reduce(const PTask &t, double (&v)[NV], d
   return true;
 }
 
-__global__ void __launch_bounds__(kRealThreads, 3)
+__global__ void __launch_bounds__(kRealThreads, 2)
     gemm_f64_kernel(const GBlock *__restrict__ blocks, const PTask *__restrict__ tasks, int ntasks,
                     double *__restrict__ C, const double *__restrict__ A, const double *__restrict__ B,
                     double alpha, double beta, double *__restrict__ part, int *__restrict__ pcnt, int base_ok) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   SmemR &s = *reinterpret_cast<SmemR *>(smem_raw);
   __shared__ int ticket;
+  PL_STAMP(0);
   pdl_wait();  // operands, output and the split-K counters belong to earlier kernels too
   pdl_trigger();
+  PL_STAMP(1);
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int wm = warp & 1, wn = warp >> 1;
   const int g = lane >> 2, t = lane & 3;
-  for (int ti = blockIdx.x; ti < ntasks; ti += gridDim.x) {
+  [[maybe_unused]] int ntask = 0;
+  for (int ti = blockIdx.x; ti < ntasks; ti += gridDim.x, ++ntask) {
     const PTask task = tasks[ti];
     const GBlock b = blocks[task.block];
     const int64_t m0 = task.m0, n0 = task.n0;
     const int vec = vec_flags(b, base_ok);
-    double acc[32];
+    // two accumulator sets, one per K sub-step of 8 in a stage (the 16 DMMA of a stage are
+    // independent); their sum is (sub-step 0) + (sub-step 8)
+    double acc[32], acc2[32];
 #pragma unroll
-    for (int q = 0; q < 32; ++q) acc[q] = 0.0;
+    for (int q = 0; q < 32; ++q) acc[q] = acc2[q] = 0.0;
     if (task.kind == 0 && task.ke > task.kb) {
-      k_loop(task.kb, task.ke,
+      k_loop<NST>(task.kb, task.ke,
              [&](int st, int64_t k0) { load_tiles_r(s, st, b, A, B, m0, n0, k0, vec); },
              [&](int st) {
                // the warp's 32×32 as 2 × 4 blocks of 16×8 (m16n8k8), K in steps of 8
 #pragma unroll
                for (int kk = 0; kk < BK; kk += 8) {
+                 double *ac = kk == 0 ? acc : acc2;
                  double af[2][4], bf[4][2];
 #pragma unroll
                  for (int mi = 0; mi < 2; ++mi) {
@@ -247,11 +282,19 @@ __global__ void __launch_bounds__(kRealThreads, 3)
                  for (int mi = 0; mi < 2; ++mi)
 #pragma unroll
                    for (int ni = 0; ni < 4; ++ni)
-                     dmma16(*reinterpret_cast<double(*)[4]>(&acc[(mi * 4 + ni) * 4]), af[mi], bf[ni]);
+                     dmma16(*reinterpret_cast<double(*)[4]>(&ac[(mi * 4 + ni) * 4]), af[mi], bf[ni]);
                }
              });
+#pragma unroll
+      for (int q = 0; q < 32; ++q) acc[q] += acc2[q];
     }
-    if (!splitk_reduce<32, kRealThreads>(task, acc, part, pcnt, &ticket)) continue;
+    if (ntask == 0) PL_STAMP(2);
+    const bool fin = splitk_reduce<32, kRealThreads>(task, acc, part, pcnt, &ticket);
+    if (ntask == 0) {
+      PL_STAMP(3);
+      PL_SET(6, 2ull * task.nsplit + (fin ? 1 : 0));
+    }
+    if (!fin) continue;
     // epilogue: C = α·acc + β·C, in four row groups of 8 (the old values of a group are loaded
     // before its first store). Row group R, value q (column block q/2, column 2t + q%2) is
     // acc[((R/2)·4 + q/2)·4 + (R%2)·2 + q%2] (the m16n8k8 fragments)
@@ -275,6 +318,8 @@ __global__ void __launch_bounds__(kRealThreads, 3)
       }
     }
   }
+  PL_SET(5, ntask);
+  PL_STAMP(4);
 }
 
 // ---- complex ---------------------------------------------------------------------------
@@ -351,7 +396,7 @@ __global__ void __launch_bounds__(kCplxThreads, 2)
 #pragma unroll
     for (int q = 0; q < 32; ++q) acc[q] = 0.0;
     if (task.kind == 0 && task.ke > task.kb) {
-      k_loop(task.kb, task.ke, [&](int st, int64_t k0) { load_tiles_c(s, st, b, A, B, m0, n0, k0); },
+      k_loop<NST>(task.kb, task.ke, [&](int st, int64_t k0) { load_tiles_c(s, st, b, A, B, m0, n0, k0); },
              [&](int st) {
 #pragma unroll
                for (int kk = 0; kk < BK; kk += 4) {
@@ -657,7 +702,7 @@ int tkb_gemm_plain_prepare(tkb_ctx *ctx, tkb_plan *p, const std::vector<GTile> &
     if (e == cudaSuccess) e = cudaMemcpy(p->ptasks, tasks.data(), tasks.size() * sizeof(PTask), cudaMemcpyHostToDevice);
   }
   if (e == cudaSuccess && nslots > 0) {
-    e = cudaMalloc((void **)&p->part, (size_t)npart * 32 * threads * sizeof(double));
+    e = cudaMalloc((void **)&p->part, (size_t)npart * BM * BN * (cplx ? 2 : 1) * sizeof(double));
     if (e == cudaSuccess) e = cudaMalloc((void **)&p->pcnt, nslots * sizeof(int));
     if (e == cudaSuccess) e = cudaMemset(p->pcnt, 0, nslots * sizeof(int));
   }
@@ -692,3 +737,12 @@ int tkb_gemm_launch(tkb_ctx *ctx, const tkb_plan *p, void *C, const void *A, con
   TKB_CUDA_TRY(ctx, cudaGetLastError());
   return TKB_OK;
 }
+
+#ifdef TKB_TIMELINE
+// copies the plain kernel's per-CTA stamps out (kPlTlCtas × kPlTlSlots values) and clears them
+extern "C" int tkb_timeline_read_plain(unsigned long long *out) {
+  if (cudaMemcpyFromSymbol(out, tkb_tl_plain, sizeof(tkb_tl_plain)) != cudaSuccess) return -1;
+  static unsigned long long zero[kPlTlCtas * kPlTlSlots];
+  return cudaMemcpyToSymbol(tkb_tl_plain, zero, sizeof(tkb_tl_plain)) == cudaSuccess ? kPlTlSlots : -1;
+}
+#endif
