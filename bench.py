@@ -430,6 +430,34 @@ def whole_job_value(flops_per_step, world, steps, ms):
     return flops_per_step * world * steps / (ms * 1e-3) / 1e9
 
 
+def parse_cpulist(text):
+    """CPU numbers of a sysfs cpulist such as "0-27,56-83"."""
+    cpus = set()
+    for part in text.strip().split(","):
+        if part:
+            a, _, b = part.partition("-")
+            cpus.update(range(int(a), int(b or a) + 1))
+    return cpus
+
+
+def gpu_numa_cpus(dev_index):
+    """(NUMA node, its CPUs this process may use) for the node the GPU's PCIe function sits on,
+    from sysfs; (None, None) where the system does not say."""
+    import torch
+    try:
+        p = torch.cuda.get_device_properties(dev_index)
+        bdf = f"{p.pci_domain_id:04x}:{p.pci_bus_id:02x}:{p.pci_device_id:02x}.0"
+        with open(f"/sys/bus/pci/devices/{bdf}/numa_node") as f:
+            node = int(f.read().strip())
+        if node < 0:
+            return None, None
+        with open(f"/sys/devices/system/node/node{node}/cpulist") as f:
+            cpus = parse_cpulist(f.read()) & os.sched_getaffinity(0)
+        return (node, cpus) if cpus else (None, None)
+    except (OSError, ValueError, AttributeError):
+        return None, None
+
+
 def run_ours(args):
     import numpy as np
     import torch
@@ -523,9 +551,18 @@ def run_ours(args):
     # step. Steps are pipelined the way a serving loop would run them: two captured instances of
     # the contraction alternate, the inputs of step i+1 go up and the result of step i-1 comes
     # back on their own streams (the copy engines) while step i computes.
-    host_in = {k: torch.from_numpy(np.ascontiguousarray(v.data)).pin_memory() for k, v in tens_o.items()}
-    nout = plans["split"].output.data.numel()
-    host_out = [torch.empty(nout, dtype=torch.float64).pin_memory() for _ in range(2)]
+    # the pinned staging buffers get their pages on the GPU's NUMA node (the allocating thread runs
+    # there meanwhile), so the copy engines do not read them across the socket link
+    numa_node, near = gpu_numa_cpus(local)
+    saved_cpus = os.sched_getaffinity(0)
+    if near:
+        os.sched_setaffinity(0, near)
+    try:
+        host_in = {k: torch.from_numpy(np.ascontiguousarray(v.data)).pin_memory() for k, v in tens_o.items()}
+        nout = plans["split"].output.data.numel()
+        host_out = [torch.empty(nout, dtype=torch.float64).pin_memory() for _ in range(2)]
+    finally:
+        os.sched_setaffinity(0, saved_cpus)
     h2d = sum(v.numel() * v.element_size() for v in host_in.values())
     d2h = host_out[0].numel() * host_out[0].element_size()
     twin = tk.NetworkPlan(expr, precision="split", **{k: to_device(v, dev) for k, v in tens_o.items()})
@@ -648,6 +685,7 @@ def run_ours(args):
                 "max_rel_err": err,
                 "e2e": {"value": e2e_value, "unit": "GFLOP/s", "h2d_bytes_per_step": h2d,
                         "d2h_bytes_per_step": d2h, "ms_per_step": ms_e2e / args.steps,
+                        "host_buffers_numa_node": numa_node,
                         "pipelined": "inputs of step i+1 up and result of step i-1 back on copy streams "
                                      "while step i computes (two captured instances)"},
                 "e2e_serial": {"value": whole_job_value(flops, world, args.steps, ms_serial), "unit": "GFLOP/s",
