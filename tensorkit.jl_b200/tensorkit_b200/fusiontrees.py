@@ -5,6 +5,9 @@ Follows, for multiplicity-free sectors (U1, SU2, U1⊠SU2):
 - the deterministic iteration order (`src/fusiontrees/iterator.jl:98-226`);
 - `bendright` / `bendleft` and `repartition` (`src/fusiontrees/duality_manipulations.jl:33-194`,
   `:460-505`);
+- `multi_Fmove` / `multi_Fmove_inv` (`src/fusiontrees/basic_manipulations.jl:191-440`), `foldright` /
+  `foldleft`, `cycleclockwise` / `cycleanticlockwise` and `fstranspose`
+  (`src/fusiontrees/duality_manipulations.jl:220-426`, `:534-562`);
 - `artin_braid` for single trees (`src/fusiontrees/braiding_manipulations.jl:18-79`) and for
   blocks (`:81-198`), `braid` of a unique-fusion tree (`:215-251`), `fsbraid` (`:304-340`);
 - `linearizepermutation` and `permutation2swaps` (`src/auxiliary/auxiliary.jl:1-28`).
@@ -19,12 +22,13 @@ from functools import lru_cache
 
 import numpy as np
 
-from .sectors import (Bsymbol, Fsymbol, Nsymbol, Rsymbol, frobenius_schur_phase,
+from .sectors import (Asymbol, Bsymbol, Fsymbol, Nsymbol, Rsymbol, frobenius_schur_phase,
                       invsqrtdim, otimes_many, sqrtdim)
 
 __all__ = ["FusionTree", "FusionTreeBlock", "fusiontrees", "bendright", "bendleft", "split",
            "repartition", "artin_braid", "braid", "permute", "linearizepermutation",
-           "permutation2swaps"]
+           "permutation2swaps", "multi_Fmove", "multi_Fmove_inv", "foldright", "foldleft",
+           "cycleclockwise", "cycleanticlockwise", "fstranspose"]
 
 
 class FusionTree:
@@ -256,6 +260,188 @@ def repartition(src, N):
         dst, ct = f(dst)
         coeff = ct * coeff
     return dst, coeff
+
+
+# ------------------------------------------------------------------------------------
+# folding, cyclic permutations and transpose
+# ------------------------------------------------------------------------------------
+def _extend(T, u, isdual_u, coupled):
+    """T with one more leg u on the right, the old coupled line fused with u to `coupled`."""
+    inner = (T.innerlines + (T.coupled,)) if len(T.uncoupled) >= 2 else ()
+    return FusionTree(T.uncoupled + (u,), coupled, T.isdual + (isdual_u,), inner)
+
+
+def multi_Fmove(f):
+    """Recouple the splitting tree f so that its first leg a meets the coupled line last:
+    a list of (f′, coeff), f′ the trees of the other legs (coupled b, a ⊗ b → f.coupled on
+    top). One F-move per further leg, from the left: after legs 0..k-1 the state is
+    (a ⊗ T → e) with e the coupling of those legs in f; adding leg k (fused to d in f) gives
+    Σ_b′ [F^{a b u}_d]^e_{b′} a ⊗ (T ⊗ u → b′) → d (`basic_manipulations.jl:191-322`)."""
+    N = len(f.uncoupled)
+    if N == 0:
+        raise ValueError("multi_Fmove requires at least one uncoupled sector")
+    c = f.coupled
+    if N == 1:
+        return [(FusionTree((), c.unit(), (), ()), 1.0)]
+    a = f.uncoupled[0]
+    ext = tuple(f.innerlines) + (c,)  # ext[k-2]: the line the first k legs fuse to in f
+    u1 = f.uncoupled[1]
+    states = [(FusionTree((u1,), u1, (f.isdual[1],), ()), 1.0)]
+    for k in range(2, N):
+        e, d, u = ext[k - 2], ext[k - 1], f.uncoupled[k]
+        nxt = []
+        for T, cf in states:
+            b = T.coupled
+            for b2 in b.otimes(u):
+                if not Nsymbol(a, b2, d):
+                    continue
+                F = Fsymbol(a, b, u, d, e, b2)
+                if F != 0.0:
+                    nxt.append((_extend(T, u, f.isdual[k], b2), cf * F))
+        states = nxt
+    return states
+
+
+def multi_Fmove_inv(a, c, f, isduala=False):
+    """Fuse a new first leg a (duality flag isduala) with the splitting tree f (coupled b) to
+    c, expanded in standard trees of (a, f's legs) → c: a list of (tree, coeff). The last leg
+    v of f is peeled off with the inverse F-move a ⊗ (b′ ⊗ v → b) → c = Σ_e [F^{a b′ v}_c]^e_b
+    (a ⊗ b′ → e) ⊗ v → c (F is orthogonal for these sectors), then the rest recursively
+    (`basic_manipulations.jl:353-440`)."""
+    b = f.coupled
+    if not Nsymbol(a, b, c):
+        raise ValueError(f"cannot fuse sectors {a} and {b} to {c}")
+    N = len(f.uncoupled)
+    if N == 0:
+        return [(FusionTree((a,), c, (isduala,), ()), 1.0)]
+    if N == 1:
+        return [(FusionTree((a, f.uncoupled[0]), c, (isduala, f.isdual[0]), ()), 1.0)]
+    v = f.uncoupled[-1]
+    bp = f.innerlines[-1] if N > 2 else f.uncoupled[0]
+    fp = FusionTree(f.uncoupled[:-1], bp, f.isdual[:-1], f.innerlines[:-1] if N > 2 else ())
+    out = []
+    for e in a.otimes(bp):
+        if not Nsymbol(e, v, c):
+            continue
+        F = Fsymbol(a, bp, v, c, e, b)
+        if F == 0.0:
+            continue
+        for S, cf in multi_Fmove_inv(a, e, fp, isduala):
+            out.append((_extend(S, v, f.isdual[-1], c), cf * F))
+    return out
+
+
+def _fold_terms(fa, fo, right):
+    """Terms of folding the first leg a of the tree fa (splitting side for foldright, fusion
+    side for foldleft) onto the other tree fo: ((f₁′, f₂′), coeff) pairs with coefficient
+    √d_c/√d_b · A^{ab}_c · (multi_Fmove coefficient) · (multi_Fmove_inv coefficient), times
+    χ_a when a is a dual leg (`duality_manipulations.jl:220-236`, `:319-325`)."""
+    a, isduala, c = fa.uncoupled[0], fa.isdual[0], fa.coupled
+    ka = frobenius_schur_phase(a)
+    acc = {}
+    for fap, ca in multi_Fmove(fa):
+        b = fap.coupled
+        A = Asymbol(a, b, c)
+        if A == 0.0:
+            continue
+        c0 = sqrtdim(c) * invsqrtdim(b) * A * ca
+        for fop, co in multi_Fmove_inv(a.dual(), b, fo, not isduala):
+            coeff = c0 * co * (ka if isduala else 1.0)
+            key = (fap, fop) if right else (fop, fap)
+            acc[key] = acc.get(key, 0.0) + coeff
+    return acc
+
+
+def _fold(src, right):
+    if not isinstance(src, FusionTreeBlock):
+        f1, f2 = src
+        acc = _fold_terms(f1, f2, True) if right else _fold_terms(f2, f1, False)
+        if len(acc) != 1:
+            raise ValueError("folding a tree pair needs unique fusion; use a FusionTreeBlock")
+        (pair, coeff), = acc.items()
+        return pair, coeff
+    u1, u2 = src.uncoupled
+    d1, d2 = src.isdual
+    unit = (u1 + u2)[0].unit()
+    if right:
+        if not u1:
+            raise ValueError("foldright needs a splitting leg")
+        dst = FusionTreeBlock((u1[1:], (u1[0].dual(),) + u2), (d1[1:], (not d1[0],) + d2), unit)
+    else:
+        if not u2:
+            raise ValueError("foldleft needs a fusion leg")
+        dst = FusionTreeBlock(((u2[0].dual(),) + u1, u2[1:]), ((not d2[0],) + d1, d2[1:]), unit)
+    U = np.zeros((len(dst), len(src)))
+    for col, (f1, f2) in enumerate(src.trees):
+        acc = _fold_terms(f1, f2, True) if right else _fold_terms(f2, f1, False)
+        for pair, coeff in acc.items():
+            U[dst.index[pair], col] += coeff
+    return dst, U
+
+
+def foldright(src):
+    """Fold the first splitting leg a to the fusion side (it becomes the first fusion leg,
+    dualised): (dst, U) for a block, (pair, coeff) for a unique-fusion tree pair
+    (`duality_manipulations.jl:220-290`)."""
+    return _fold(src, True)
+
+
+def foldleft(src):
+    """Fold the first fusion leg to the splitting side (`duality_manipulations.jl:316-376`)."""
+    return _fold(src, False)
+
+
+def _compose(first, second):
+    (tmp, U1) = first
+    dst, U2 = second(tmp)
+    return dst, (U2 @ U1 if isinstance(U1, np.ndarray) else U2 * U1)
+
+
+def _numout(src):
+    return src.numout() if isinstance(src, FusionTreeBlock) else len(src[0])
+
+
+def _numin(src):
+    return src.numin() if isinstance(src, FusionTreeBlock) else len(src[1])
+
+
+def cycleclockwise(src):
+    """Fold the first splitting leg to the fusion side and bend the last fusion leg back: the
+    legs rotate one step clockwise at fixed (N₁, N₂) (`duality_manipulations.jl:402-411`)."""
+    if _numout(src) > 0:
+        return _compose(foldright(src), bendleft)
+    return _compose(bendleft(src), foldright)
+
+
+def cycleanticlockwise(src):
+    """Bend the last splitting leg to the fusion side and fold the first fusion leg back
+    (`duality_manipulations.jl:433-442`)."""
+    if _numin(src) > 0:
+        return _compose(foldleft(src), bendright)
+    return _compose(bendright(src), foldleft)
+
+
+def fstranspose(src, p1, p2):
+    """Planar (cyclic) permutation (p₁, p₂), 1-based, as a repartition followed by cyclic
+    rotations, the shorter way round (`duality_manipulations.jl:534-562`)."""
+    p1, p2 = tuple(p1), tuple(p2)
+    N1 = len(p1)
+    N = N1 + len(p2)
+    p = linearizepermutation(p1, p2, _numout(src), _numin(src))
+    dst, U = repartition(src, N1)
+    if len(p) == 0:
+        return dst, U
+    i1 = p.index(1) + 1
+    if i1 == 1:
+        return dst, U
+    Nhalf = N >> 1
+    while 1 < i1 <= Nhalf:
+        dst, U = _compose((dst, U), cycleanticlockwise)
+        i1 -= 1
+    while Nhalf < i1:
+        dst, U = _compose((dst, U), cycleclockwise)
+        i1 = (i1 % N) + 1
+    return dst, U
 
 
 # ------------------------------------------------------------------------------------

@@ -22,7 +22,7 @@ from . import _lib as L
 from .backend import DeviceTable, get_context
 from .spaces import SpaceMismatch
 from .tensor import AdjointTensorMap, TensorMap, new_tensor
-from .treetransformers import flatten_transformer, treebraider
+from .treetransformers import flatten_transformer, treebraider, treetransposer
 
 __all__ = ["permute", "permute_", "braid", "braid_", "add_transform_", "transpose",
            "transpose_", "repartition", "device_table", "dtype_code"]
@@ -66,13 +66,17 @@ def _norm_p(p):
     return (tuple(int(i) for i in p[0]), tuple(int(i) for i in p[1]))
 
 
-def device_table(ctx, tdst_space, tsrc, p, levels):
+def device_table(ctx, tdst_space, tsrc, p, levels, planar=False):
+    """The device table of braid!(…, p, levels), or of transpose!(…, p) with `planar`."""
     parent_space = tsrc.parent.space if isinstance(tsrc, AdjointTensorMap) else None
     src_len = tsrc.parent.space.dim() if parent_space is not None else tsrc.space.dim()
-    key = ("braid", tdst_space, tsrc.space, p, levels, parent_space)
+    key = ("transpose" if planar else "braid", tdst_space, tsrc.space, p, levels, parent_space)
 
     def make():
-        tr = treebraider(tdst_space, tsrc.space, p, levels, parent_space)
+        if planar:
+            tr = treetransposer(tdst_space, tsrc.space, p, parent_space)
+        else:
+            tr = treebraider(tdst_space, tsrc.space, p, levels, parent_space)
         flat = flatten_transformer(tr, p)
         return DeviceTable(ctx, flat, src_len, tdst_space.dim())
 
@@ -161,14 +165,19 @@ def braid(t, p, levels, copy=False):
 
 
 def transpose_(tdst, tsrc, p, alpha=1.0, beta=0.0):
-    """Cyclic permutation; for bosonic sectors identical to permute!."""
+    """tdst = β·tdst + α·transpose(tsrc, p): a cyclic (planar) permutation, whose trees move by
+    folds, bends and rotations only (`src/tensors/indexmanipulations.jl:378-391`)."""
     from .fusiontrees import linearizepermutation
     p = _norm_p(p)
     lin = linearizepermutation(p[0], p[1], tsrc.numout(), tsrc.numin())
     n = len(lin)
     if n and not all(lin[(i + 1) % n] == (lin[i] % n) + 1 for i in range(n)):
         raise ValueError(f"invalid cyclic or planar permutation p = {p}")
-    return permute_(tdst, tsrc, p, alpha, beta)
+    if tsrc.space.permute(p) != tdst.space:
+        raise SpaceMismatch(f"tsrc = {tsrc.space}, tdst = {tdst.space}, p = {p}")
+    ctx = get_context(tdst.data.device.index)
+    table = device_table(ctx, tdst.space, tsrc, p, None, planar=True)
+    return add_transform_(tdst, tsrc, p, table, alpha, beta)
 
 
 def transpose(t, p=None, copy=False):

@@ -387,6 +387,16 @@ def Bsymbol(a, b, c):
     return (sqrtdim(a) * sqrtdim(b) * invsqrtdim(c)) * Fsymbol(a, b, b.dual(), a, c, a.unit())
 
 
+def Asymbol(a, b, c):
+    """A^{ab}_c = sqrtdim(a)*sqrtdim(b)*invsqrtdim(c) * χ_ā * F^{ā a b}_b[1, c] (the folding
+    coefficient; `docs/src/appendix/categories.md:590-593`, real for these sectors)."""
+    if a.fusionstyle == "unique":
+        return 1.0 if Nsymbol(a, b, c) else 0.0
+    ad = a.dual()
+    return ((sqrtdim(a) * sqrtdim(b) * invsqrtdim(c)) * frobenius_schur_phase(ad)
+            * Fsymbol(ad, a, b, b, a.unit(), c))
+
+
 def otimes_many(sectors, unit):
     """All coupled sectors of a tuple of sectors, as a list of unique values."""
     if len(sectors) == 0:

@@ -18,9 +18,10 @@ from __future__ import annotations
 import numpy as np
 
 from .fusiontrees import braid as _braid_trees
+from .fusiontrees import fstranspose as _fstranspose
 from .structure import fusionblocks, sectorstructure, subblockstructure
 
-__all__ = ["AbelianTreeTransformer", "GenericTreeTransformer", "treebraider", "FlatTable",
+__all__ = ["AbelianTreeTransformer", "GenericTreeTransformer", "treebraider", "treetransposer", "FlatTable",
            "flatten_transformer"]
 
 
@@ -56,9 +57,16 @@ def _adjoint_subblocks(Wparent):
     return out
 
 
-def build_transformer(Vdst, Vsrc, p, levels, src_adjoint_of=None):
-    """Build the transformer for braid!(tdst, tsrc, p, levels); `src_adjoint_of` is the
-    parent HomSpace when the source is a lazy adjoint (then Vsrc == adjoint(parent))."""
+def build_transformer(Vdst, Vsrc, p, levels, src_adjoint_of=None, planar=False):
+    """Build the transformer for braid!(tdst, tsrc, p, levels), or with `planar` for
+    transpose!(tdst, tsrc, p) (trees moved by fstranspose, levels unused); `src_adjoint_of` is
+    the parent HomSpace when the source is a lazy adjoint (then Vsrc == adjoint(parent))."""
+    if planar:
+        def move(x):
+            return _fstranspose(x, p[0], p[1])
+    else:
+        def move(x):
+            return _braid_trees(x, p, levels)
     if Vsrc.permute(p) != Vdst:
         from .spaces import SpaceMismatch
         raise SpaceMismatch("Incompatible spaces for permuting.")
@@ -70,12 +78,12 @@ def build_transformer(Vdst, Vsrc, p, levels, src_adjoint_of=None):
     if _is_unique(Vsrc):
         data = []
         for pair in sectorstructure(Vsrc).fusiontrees:
-            pdst, coeff = _braid_trees(pair, p, levels)
+            pdst, coeff = move(pair)
             data.append((coeff, fts_dst[pdst], fts_src[pair]))
         return AbelianTreeTransformer(data)
     data = []
     for blk in fusionblocks(Vsrc):
-        dst, U = _braid_trees(blk, p, levels)
+        dst, U = move(blk)
         sz_src = fts_src[blk.trees[0]][0]
         sz_dst = fts_dst[dst.trees[0]][0]
         ss = [(fts_src[t][1], fts_src[t][2]) for t in blk.trees]
@@ -96,6 +104,20 @@ def treebraider(Vdst, Vsrc, p, levels, src_adjoint_of=None):
     t = _TRANSFORMER_CACHE.get(key)
     if t is None:
         t = build_transformer(Vdst, Vsrc, p, levels, src_adjoint_of)
+        if len(_TRANSFORMER_CACHE) > 10000:
+            _TRANSFORMER_CACHE.clear()
+        _TRANSFORMER_CACHE[key] = t
+    return t
+
+
+def treetransposer(Vdst, Vsrc, p, src_adjoint_of=None):
+    """Transformer of transpose!(tdst, tsrc, p): the trees move by fstranspose (folds, bends
+    and cyclic rotations, no braiding), cached per `(Vdst, Vsrc, p)`
+    (`src/tensors/treetransformers.jl:175-180`)."""
+    key = ("transpose", Vdst, Vsrc, tuple(map(tuple, p)), src_adjoint_of)
+    t = _TRANSFORMER_CACHE.get(key)
+    if t is None:
+        t = build_transformer(Vdst, Vsrc, p, ((), ()), src_adjoint_of, planar=True)
         if len(_TRANSFORMER_CACHE) > 10000:
             _TRANSFORMER_CACHE.clear()
         _TRANSFORMER_CACHE[key] = t
