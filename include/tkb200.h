@@ -209,11 +209,10 @@ int tkb_reduce_async(tkb_ctx *ctx, const tkb_rplan *plan, int kind, int dtype,
  * process exits. The caller passes the data vectors and host segment arrays (same meaning
  * as tkb_rplan_create) and receives (re, im) in host_out after the stream has completed.
  * Limits: at most 1024 segments (TKB_ERR_SIZE beyond that). The first call on a device
- * looks up the array's device address for that device; make that first call before any
- * stream capture. With CUDA's lazy module loading that first call also loads the library's
- * kernels onto the device, which can itself need device memory: make it once per device at
- * start-up (any valid call that reduces at least one element), not first from an
- * out-of-memory recovery path. Host-side staging uses a few KiB of the caller's stack. All
+ * looks up the array's device address for that device and, with CUDA's lazy module
+ * loading, loads the library's kernels onto the device, which can itself need device
+ * memory: make it once per device at start-up (any valid call that reduces at least one
+ * element), not first from an out-of-memory recovery path. Host-side staging uses a few KiB of the caller's stack. All
  * calls share the array, so calls that overlap on the GPU (other streams, other host threads)
  * race and must be serialised by the caller. */
 int tkb_reduce_noalloc(int device, void *stream, int kind, int dtype, const void *x,
