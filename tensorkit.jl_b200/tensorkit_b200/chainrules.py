@@ -12,7 +12,8 @@ Restates `ext/TensorKitChainRulesCoreExt/tensoroperations.jl` and `src/pullbacks
 - `rrule_tensortrace` (`:152-199`): dA = ΔC ⊗ id(traced legs), permuted back, times
   conj(α) (α when conjA).
 - `rrule_permute` (`src/pullbacks/indexmanipulations.jl:1-31`, `ext/.../linalg.jl:62-70`):
-  the inverse permutation with conj(α).
+  the inverse permutation with conj(α); `rrule_transpose` (`ext/.../linalg.jl:72-81`): the
+  inverse cyclic permutation, through transpose! again.
 - `rrule_tr`: Δ ↦ conj(Δ)·id;  `rrule_norm`: Δ ↦ (Δ/‖t‖)·t.
 
 All adjoints run on the forward kernels: the transpose transform reads its source with the
@@ -33,7 +34,8 @@ from .tensoroperations import (_alloc, _pairwise_steps, parse_tensor_expr, tenso
                                tensoradd_structure, tensorcontract, tensorcontract_,
                                tensorcontract_structure)
 
-__all__ = ["rrule_tensorcontract", "rrule_tensoradd", "rrule_tensortrace", "rrule_permute", "rrule_tr",
+__all__ = ["rrule_tensorcontract", "rrule_tensoradd", "rrule_tensortrace", "rrule_permute", "rrule_transpose",
+           "rrule_tr",
            "rrule_norm",
            "network_with_pullback", "TensorContract"]
 
@@ -166,6 +168,25 @@ def rrule_permute(t, p, alpha=1.0):
         pdA = _rep(ip, t.numout())
         dA = new_tensor(dC.space.permute(pdA), dC.data.dtype, dC.data.device)
         permute_(dA, dC, pdA, _conj(alpha), 0.0)
+        return dA
+
+    return out, pullback
+
+
+def rrule_transpose(t, p=None):
+    """transpose(t, p) (a cyclic permutation; default (reverse(domain), reverse(codomain)))
+    and its pullback: transpose of the cotangent by the inverse permutation, split like t
+    (`ext/TensorKitChainRulesCoreExt/linalg.jl:72-81`)."""
+    from .indexmanipulations import transpose, transpose_
+    if p is None:
+        p = (tuple(reversed(t.domainind())), tuple(reversed(t.codomainind())))
+    p = (tuple(p[0]), tuple(p[1]))
+    out = transpose(t, p, copy=True)
+
+    def pullback(dC):
+        pdA = _rep(_invperm(_lin(p)), t.numout())
+        dA = new_tensor(dC.space.permute(pdA), dC.data.dtype, dC.data.device)
+        transpose_(dA, dC, pdA, 1.0, 0.0)
         return dA
 
     return out, pullback

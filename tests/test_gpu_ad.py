@@ -90,6 +90,20 @@ def test_permute_pullback_is_inverse_permute():
     assert abs(lhs - rhs) <= 1e-12 * abs(lhs)
 
 
+@pytest.mark.parametrize("p", [None, ((2, 3), (1,)), ((3,), (2, 1)), ((1,), (3, 2)), ((), (2, 1, 3)), ((3, 1, 2), ())])
+def test_transpose_pullback_is_adjoint(p):
+    """<dC, transpose(t, p)> = <pullback(dC), t> for cyclic p (the pullback transposes back)."""
+    V, Pp = cfg5_spaces()
+    t = to_device(O.randn(O.Hom([V, Pp], [V]), 9, True))
+    out, pb = CR.rrule_transpose(t, p)
+    dC = to_device(O.randn(from_hom(out.space), 10, True))
+    dA = pb(dC)
+    assert dA.space == t.space
+    lhs = tk.inner(dC, out)
+    rhs = tk.inner(dA, t)
+    assert abs(lhs - rhs) <= 1e-12 * abs(lhs)
+
+
 def test_torch_autograd_bridge():
     V, Pp = cfg5_spaces()
     A = to_device(O.randn(O.Hom([V, Pp], [V]), 1, True))
