@@ -16,7 +16,7 @@ from .tensor import TensorMap, AdjointTensorMap
 from .backend import (get_context, set_precision, using_precision, precision, B200Backend,
                       empty_globalcaches, launch_count)
 from .indexmanipulations import (permute, permute_, braid, braid_, transpose, transpose_,
-                                 repartition, add_transform_)
+                                 repartition, add_transform_, flip)
 from .linalg import mul_, compose, norm, tr, inner, dot, scale_, add_
 from .tensoroperations import (tensoradd_, tensorcontract_, tensorcontract, contract_,
                                tensor, tensorcontract_structure, tensoradd_structure,

@@ -28,7 +28,7 @@ from .sectors import (Asymbol, Bsymbol, Fsymbol, Nsymbol, Rsymbol, frobenius_sch
 __all__ = ["FusionTree", "FusionTreeBlock", "fusiontrees", "bendright", "bendleft", "split",
            "repartition", "artin_braid", "braid", "permute", "linearizepermutation",
            "permutation2swaps", "multi_Fmove", "multi_Fmove_inv", "foldright", "foldleft",
-           "cycleclockwise", "cycleanticlockwise", "fstranspose"]
+           "cycleclockwise", "cycleanticlockwise", "fstranspose", "flip"]
 
 
 class FusionTree:
@@ -442,6 +442,32 @@ def fstranspose(src, p1, p2):
         dst, U = _compose((dst, U), cycleclockwise)
         i1 = (i1 % N) + 1
     return dst, U
+
+
+def _flip_tree(f, i, factor_if):
+    isd = list(f.isdual)
+    fac = frobenius_schur_phase(f.uncoupled[i]) if factor_if(isd[i]) else 1.0
+    isd[i] = not isd[i]
+    return FusionTree(f.uncoupled, f.coupled, isd, f.innerlines), fac
+
+
+def flip(pair, I, inv=False):
+    """Flip the duality flags of the legs I (1-based, splitting legs first) of a tree pair:
+    ((f₁′, f₂′), factor). For bosonic sectors (θ = 1) each flipped leg a contributes χ_a when
+    it was dual (χ_a when it was not, with `inv`), else 1; the labels stay
+    (`src/fusiontrees/braiding_manipulations.jl:388-436`)."""
+    f1, f2 = pair
+    n1 = len(f1.uncoupled)
+    factor = 1.0
+    for i in I:
+        if not 1 <= i <= n1 + len(f2.uncoupled):
+            raise IndexError(f"flip: leg {i} out of range")
+        if i <= n1:
+            f1, fac = _flip_tree(f1, i - 1, (lambda d: not d) if inv else (lambda d: d))
+        else:
+            f2, fac = _flip_tree(f2, i - n1 - 1, (lambda d: not d) if inv else (lambda d: d))
+        factor *= fac
+    return (f1, f2), factor
 
 
 # ------------------------------------------------------------------------------------

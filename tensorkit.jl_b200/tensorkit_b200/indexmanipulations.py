@@ -22,7 +22,7 @@ from . import _lib as L
 from .backend import DeviceTable, get_context
 from .spaces import SpaceMismatch
 from .tensor import AdjointTensorMap, TensorMap, new_tensor
-from .treetransformers import flatten_transformer, treebraider, treetransposer
+from .treetransformers import flatten_transformer, treebraider, treeflipper, treetransposer
 
 __all__ = ["permute", "permute_", "braid", "braid_", "add_transform_", "transpose",
            "transpose_", "repartition", "device_table", "dtype_code"]
@@ -186,6 +186,28 @@ def transpose(t, p=None, copy=False):
     p = _norm_p(p)
     dst = new_tensor(t.space.permute(p), t.data.dtype, t.data.device)
     return transpose_(dst, t, p)
+
+
+def flip(t, I, inv=False):
+    """A tensor isomorphic to t with the arrows of the legs i ∈ I (1-based) flipped:
+    space(t′, i) = flip(space(t, i)), every sub-block scaled by its tree pair's flip factor;
+    `flip(flip(t, I), I, inv=True)` is t (`src/tensors/indexmanipulations.jl:21-29`). One
+    transform launch with the identity permutation."""
+    if not isinstance(t, TensorMap):
+        raise TypeError("flip takes a TensorMap (materialise a lazy adjoint first)")
+    I = (int(I),) if isinstance(I, int) else tuple(int(i) for i in I)
+    W = t.space.flip(I)
+    dst = new_tensor(W, t.data.dtype, t.data.device)
+    n1, n = t.numout(), t.numind()
+    p = (tuple(range(1, n1 + 1)), tuple(range(n1 + 1, n + 1)))
+    ctx = get_context(t.data.device.index)
+
+    def make():
+        flat = flatten_transformer(treeflipper(W, t.space, I, inv), p)
+        return DeviceTable(ctx, flat, t.space.dim(), W.dim())
+
+    table = ctx.tables.get_or(("flip", W, t.space, I, bool(inv)), make)
+    return add_transform_(dst, t, p, table, 1.0, 0.0)
 
 
 def repartition(t, N1, copy=False):

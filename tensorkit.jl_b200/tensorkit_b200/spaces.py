@@ -303,6 +303,17 @@ class HomSpace:
             raise ValueError(f"{p} is not a valid permutation for {self}")
         return self.select(p)
 
+    def flip(self, I) -> "HomSpace":
+        """The legs i ∈ I (1-based, codomain first) flipped: W′[i] = flip(W[i])."""
+        I = {int(i) for i in I}
+        n1 = len(self.codomain)
+        if not all(1 <= i <= self.numind() for i in I):
+            raise IndexError(f"flip: indices {sorted(I)} out of range for {self}")
+        cod = ProductSpace(tuple(V.flip() if k + 1 in I else V for k, V in enumerate(self.codomain)), self.unit())
+        dom = ProductSpace(tuple(V.flip() if n1 + k + 1 in I else V for k, V in enumerate(self.domain)),
+                           self.unit())
+        return HomSpace(cod, dom, self.unit())
+
     def compose(self, other: "HomSpace") -> "HomSpace":
         if self.domain != other.codomain:
             raise SpaceMismatch(f"{self.domain} ≠ {other.codomain}")

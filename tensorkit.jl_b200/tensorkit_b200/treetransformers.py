@@ -18,10 +18,13 @@ from __future__ import annotations
 import numpy as np
 
 from .fusiontrees import braid as _braid_trees
+from .fusiontrees import FusionTreeBlock
+from .fusiontrees import flip as _flip_pair
 from .fusiontrees import fstranspose as _fstranspose
 from .structure import fusionblocks, sectorstructure, subblockstructure
 
-__all__ = ["AbelianTreeTransformer", "GenericTreeTransformer", "treebraider", "treetransposer", "FlatTable",
+__all__ = ["AbelianTreeTransformer", "GenericTreeTransformer", "treebraider", "treetransposer", "treeflipper",
+           "FlatTable",
            "flatten_transformer"]
 
 
@@ -121,6 +124,47 @@ def treetransposer(Vdst, Vsrc, p, src_adjoint_of=None):
         if len(_TRANSFORMER_CACHE) > 10000:
             _TRANSFORMER_CACHE.clear()
         _TRANSFORMER_CACHE[key] = t
+    return t
+
+
+def treeflipper(Vdst, Vsrc, I, inv=False):
+    """Transformer of flip(t, I): every tree pair goes to the same pair with the duality flags
+    of the legs I toggled, scaled by the flip factor, under the identity permutation
+    (`src/tensors/indexmanipulations.jl:21-29`), cached per `(Vdst, Vsrc, I, inv)`."""
+    I = tuple(int(i) for i in I)
+    key = ("flip", Vdst, Vsrc, I, bool(inv))
+    t = _TRANSFORMER_CACHE.get(key)
+    if t is not None:
+        return t
+    fts_src = subblockstructure(Vsrc)
+    fts_dst = subblockstructure(Vdst)
+    if _is_unique(Vsrc):
+        data = []
+        for pair in sectorstructure(Vsrc).fusiontrees:
+            pdst, coeff = _flip_pair(pair, I, inv)
+            data.append((coeff, fts_dst[pdst], fts_src[pair]))
+        t = AbelianTreeTransformer(data)
+    else:
+        n1 = Vsrc.numout()
+        data = []
+        for blk in fusionblocks(Vsrc):
+            d1 = tuple((not d) if k + 1 in I else d for k, d in enumerate(blk.isdual[0]))
+            d2 = tuple((not d) if n1 + k + 1 in I else d for k, d in enumerate(blk.isdual[1]))
+            dst = FusionTreeBlock(blk.uncoupled, (d1, d2), blk.trees[0][0].coupled.unit())
+            U = np.zeros((len(dst), len(blk)))
+            for col, pair in enumerate(blk.trees):
+                pdst, coeff = _flip_pair(pair, I, inv)
+                U[dst.index[pdst], col] = coeff
+            sz_src = fts_src[blk.trees[0]][0]
+            sz_dst = fts_dst[dst.trees[0]][0]
+            ss = [(fts_src[x][1], fts_src[x][2]) for x in blk.trees]
+            sd = [(fts_dst[x][1], fts_dst[x][2]) for x in dst.trees]
+            data.append((U, (sz_dst, sd), (sz_src, ss)))
+        data.sort(key=lambda e: -(e[0].size * int(np.prod(e[1][0]))))
+        t = GenericTreeTransformer(data)
+    if len(_TRANSFORMER_CACHE) > 10000:
+        _TRANSFORMER_CACHE.clear()
+    _TRANSFORMER_CACHE[key] = t
     return t
 
 
