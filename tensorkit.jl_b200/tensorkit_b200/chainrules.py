@@ -13,7 +13,7 @@ Restates `ext/TensorKitChainRulesCoreExt/tensoroperations.jl` and `src/pullbacks
   conj(α) (α when conjA).
 - `rrule_permute` (`src/pullbacks/indexmanipulations.jl:1-31`, `ext/.../linalg.jl:62-70`):
   the inverse permutation with conj(α); `rrule_transpose` (`ext/.../linalg.jl:72-81`): the
-  inverse cyclic permutation, through transpose! again.
+  inverse cyclic permutation, through transpose! again; `rrule_flip`: flip with `inv` toggled.
 - `rrule_tr`: Δ ↦ conj(Δ)·id;  `rrule_norm`: Δ ↦ (Δ/‖t‖)·t.
 
 All adjoints run on the forward kernels: the transpose transform reads its source with the
@@ -35,7 +35,7 @@ from .tensoroperations import (_alloc, _pairwise_steps, parse_tensor_expr, tenso
                                tensorcontract_structure)
 
 __all__ = ["rrule_tensorcontract", "rrule_tensoradd", "rrule_tensortrace", "rrule_permute", "rrule_transpose",
-           "rrule_tr",
+           "rrule_flip", "rrule_tr",
            "rrule_norm",
            "network_with_pullback", "TensorContract"]
 
@@ -188,6 +188,18 @@ def rrule_transpose(t, p=None):
         dA = new_tensor(dC.space.permute(pdA), dC.data.dtype, dC.data.device)
         transpose_(dA, dC, pdA, 1.0, 0.0)
         return dA
+
+    return out, pullback
+
+
+def rrule_flip(t, I, inv=False):
+    """flip(t, I) and its pullback flip(Δ, I, inv = not inv): the flip is a ±1-signed map of
+    sub-blocks, whose adjoint is its inverse (`ext/TensorKitChainRulesCoreExt/linalg.jl`, flip rule)."""
+    from .indexmanipulations import flip
+    out = flip(t, I, inv)
+
+    def pullback(dC):
+        return flip(dC, I, not inv)
 
     return out, pullback
 

@@ -104,6 +104,20 @@ def test_transpose_pullback_is_adjoint(p):
     assert abs(lhs - rhs) <= 1e-12 * abs(lhs)
 
 
+@pytest.mark.parametrize("I", [(1,), (3,), (2, 3)])
+def test_flip_pullback_is_adjoint(I):
+    """<dC, flip(t, I)> = <pullback(dC), t> (the pullback flips back with inv toggled)."""
+    V, Pp = cfg5_spaces()
+    t = to_device(O.randn(O.Hom([V, Pp], [V]), 11, True))
+    out, pb = CR.rrule_flip(t, I)
+    dC = to_device(O.randn(from_hom(out.space), 12, True))
+    dA = pb(dC)
+    assert dA.space == t.space
+    lhs = tk.inner(dC, out)
+    rhs = tk.inner(dA, t)
+    assert abs(lhs - rhs) <= 1e-12 * abs(lhs)
+
+
 def test_torch_autograd_bridge():
     V, Pp = cfg5_spaces()
     A = to_device(O.randn(O.Hom([V, Pp], [V]), 1, True))
